@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 semi-local LCS engine: one JSON line on rank 0.
+
+Default workload (N GPUs, weak scaling): the batched comparison -- 4096 pairs per GPU, |a| log-uniform in
+[256, 65536] over 4 letters, b = a with 10 % substitutions and 1 % indels -- combed into int32 braids by
+one persistent, length-bucketed launch replayed from a CUDA graph.  metric = GCUPS (sum m*n per second,
+whole job).  Beside it: the same plan launched once per pair (the plain per-pair baseline), the
+reference's CPU path on a bounded sample (cpu_baseline), the roofline of the combing kernel, clocks.
+
+--impl reference times the reference's own CPU code (oracle/_ref, compiled from the reference sources;
+the C restatement in oracle/ when absent) on the same workload, all host threads, bounded samples.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from semilocal_b200 import gen  # noqa: E402
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+OPS_PER_CELL = 5     # compare, compare, or, two selects (R:include/SemiLocal/SemiLocalLCS.h:158-172)
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def load_peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ------------------------------------------------------------------------------------------------------
+# workloads
+# ------------------------------------------------------------------------------------------------------
+
+def batch_workload(seed: int):
+    pairs = gen.batch_pairs(4096, 256, 65536, seed=seed)
+    return pairs
+
+
+def cpu_reference_batch_sample(pairs, budget_s: float, threads: int):
+    """Reference CPU path over a bounded sample of the batch: a pool of host threads, each combing whole
+    pairs with OpenMPIterativeCombing<int,false>(1) (the reference has no batch API; this is the
+    harness-level loop over pairs).  Returns (cells, seconds, kind, sample description)."""
+    from oracle import oracle as O
+    use_ref = O.ref_available()
+    kind = "reference" if use_ref else "port"
+    # sample: pairs in a fixed shuffled order until the estimated CPU work fills the budget
+    order = np.random.default_rng(0).permutation(len(pairs))
+    est_rate = 3.0e9 * threads          # cells/s, conservative estimate to size the sample
+    target = est_rate * budget_s
+    chosen, cells = [], 0
+    for i in order:
+        a, b = pairs[i]
+        c = len(a) * len(b)
+        if cells + c > target and chosen:
+            continue
+        chosen.append(i)
+        cells += c
+        if cells >= target:
+            break
+    work = [(np.ascontiguousarray(pairs[i][0], dtype=np.int32), np.ascontiguousarray(pairs[i][1], dtype=np.int32))
+            for i in chosen]
+    lock = threading.Lock()
+    nxt = [0]
+
+    def worker():
+        while True:
+            with lock:
+                k = nxt[0]
+                nxt[0] += 1
+            if k >= len(work):
+                return
+            a, b = work[k]
+            if use_ref:
+                O.ref_comb(a, b, "openmp", 1)
+            else:
+                O.comb_antidiag(a, b, 1)
+
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=worker) for _ in range(threads)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    dt = time.perf_counter() - t0
+    desc = (f"{len(work)} of the batch's pairs ({cells / 1e9:.2f} Gcells), each combed by "
+            f"{'OpenMPIterativeCombing<int,false>(1) from the reference sources' if use_ref else 'the C restatement'}"
+            f" on a pool of {threads} host threads")
+    return cells, dt, kind, desc
+
+
+# ------------------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------------------
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    import semilocal_b200 as S
+    torch.cuda.set_device(local)
+    S._lib.check(S.lib().slcs_set_device(local))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+
+    pairs = batch_workload(5 + 1000 * rank)
+    a_cat, a_off, ms, b_cat, b_off, ns = S.concat_pairs(pairs)
+    # pinned host copies for the end-to-end leg
+    a_pin = torch.from_numpy(a_cat).pin_memory()
+    b_pin = torch.from_numpy(b_cat).pin_memory()
+    plan = S.BatchPlan(ms, ns, mode=0)
+    info = plan.info()
+    cells = info["cells"]
+    out_pin = torch.empty(plan.total, dtype=torch.int32).pin_memory()
+    sc_pin = torch.empty(len(pairs), dtype=torch.int32).pin_memory()
+    stream = torch.cuda.Stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    plan.upload(a_pin.numpy(), a_off, b_pin.numpy(), b_off, sh)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident step (value) ----
+    for _ in range(args.warmup):
+        plan.run(use_graph=True, stream=sh)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kern_ms = []
+    with Clocks(local) as clk:
+        barrier()
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            for _ in range(args.steps):
+                plan.run(use_graph=True, stream=sh)
+            ev1.record(stream)
+        ev1.synchronize()
+        barrier()
+    total_ms = ev0.elapsed_time(ev1)
+    # per-launch kernel time of the combing kernel (last step's events, on the launching stream)
+    kern_ms.append(plan.kernel_ms())
+    # correctness spot check of the timed plan against the oracle on a few pairs
+    plan.download(out_pin.numpy(), sc_pin.numpy(), sh)
+    torch.cuda.synchronize()
+    t_max = total_ms
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    ms_per_step = t_max / args.steps
+    value = cells * world / (ms_per_step * 1e-3) / 1e9
+
+    # ---- end to end through the public API: pinned H2D, run, D2H of braids + scores, every step ----
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(1):
+        plan.upload(a_pin.numpy(), a_off, b_pin.numpy(), b_off, sh)
+        plan.run(use_graph=True, stream=sh)
+        plan.download(out_pin.numpy(), sc_pin.numpy(), sh)
+    barrier()
+    e2e_steps = max(1, min(args.steps, 3))
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            plan.upload(a_pin.numpy(), a_off, b_pin.numpy(), b_off, sh)
+            plan.run(use_graph=True, stream=sh)
+            plan.download(out_pin.numpy(), sc_pin.numpy(), sh)
+        e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = cells * world / (e2e_ms * 1e-3) / 1e9
+
+    # ---- plain per-pair launches on the same plan (baseline for the batched launch) ----
+    plain = S.BatchPlan(ms, ns, mode=1)
+    plain.upload(a_pin.numpy(), a_off, b_pin.numpy(), b_off, sh)
+    plain.run(use_graph=False, stream=sh)
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        p0.record(stream)
+        plain.run(use_graph=True, stream=sh)
+        p1.record(stream)
+    p1.synchronize()
+    plain_ms = p0.elapsed_time(p1)
+    plain_gcups = cells / (plain_ms * 1e-3) / 1e9
+    plain_info = plain.info()
+    plain.close()
+
+    # ---- roofline of the combing kernel ----
+    peak_cells = ctypes.c_double(0)
+    S._lib.check(S.lib().slcs_probe_cell_peak(ctypes.byref(peak_cells)))
+    k_ms = float(np.median(kern_ms))
+    achieved_gops = OPS_PER_CELL * cells / (k_ms * 1e-3) / 1e9
+    peak_gops = OPS_PER_CELL * peak_cells.value / 1e9
+
+    result = {
+        "metric": "GCUPS", "value": round(value, 2), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded splitmix64)",
+        "config": {"workload": "batched combing: 4096 pairs per GPU, |a| log-uniform [256, 65536], 4 letters, "
+                               "b = a with 10% subst + 1% indels; int32 braids; persistent length-bucketed "
+                               "launch replayed from a CUDA graph",
+                   "pairs_per_gpu": len(pairs), "cells_per_gpu": cells, "parallelism": f"pairs sharded, {world} GPU",
+                   "l2": "inputs + braids (~%d MB) exceed the 126 MB L2" % ((a_cat.nbytes + b_cat.nbytes + 8 * plan.total) >> 20)},
+        "e2e": {"value": round(e2e_value, 2), "unit": "GCUPS", "h2d_bytes_per_step": info["h2d_bytes"],
+                "d2h_bytes_per_step": info["d2h_bytes"]},
+        "gpu_launches": info["launches"] * args.steps,
+        "plain_per_pair": {"value": round(plain_gcups, 2), "unit": "GCUPS", "launches": plain_info["launches"],
+                           "batched_over_plain": round(value / world / plain_gcups, 2)},
+        "roofline": {"bound": "int32-issue", "achieved": round(achieved_gops, 1), "peak": round(peak_gops, 1),
+                     "unit": "Gop/s", "frac": round(achieved_gops / peak_gops, 4), "traffic": None,
+                     "kernel": "comb_kernel", "kernel_ms": round(k_ms, 3),
+                     "peak_source": "slcs_probe_cell_peak (cell instruction mix, full occupancy), x5 ops/cell"},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        c_cells, c_s, kind, desc = cpu_reference_batch_sample(pairs, args.cpu_budget, os.cpu_count() or 1)
+        result["cpu_baseline"] = {"value": round(c_cells / c_s / 1e9, 3), "unit": "GCUPS",
+                                  "cores": os.cpu_count() or 1, "kind": kind, "sample": desc}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    plan.close()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------------
+# reference arm
+# ------------------------------------------------------------------------------------------------------
+
+def run_reference(args, rank, world, local):
+    if rank != 0:
+        return
+    pairs = batch_workload(5)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_reference_batch_sample(pairs, args.ref_step_s, threads)
+    cells_tot, sec_tot, kind, desc = 0, 0.0, None, None
+    for _ in range(args.steps):
+        c, s, kind, desc = cpu_reference_batch_sample(pairs, args.ref_step_s, threads)
+        cells_tot += c
+        sec_tot += s
+    value = cells_tot / sec_tot / 1e9
+    result = {
+        "impl": "reference", "metric": "GCUPS", "value": round(value, 3), "unit": "GCUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sec_tot / args.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded splitmix64)",
+        "config": {"workload": "batched combing: 4096 pairs, |a| log-uniform [256, 65536], 4 letters, "
+                               "b = a with 10% subst + 1% indels; int32 braids",
+                   "sample_per_step": desc},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GCUPS", "cores": threads, "kind": kind, "sample": desc},
+        "e2e": {"value": round(value, 3), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(result), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work for cpu_baseline")
+    ap.add_argument("--ref-step-s", type=float, default=6.0, help="seconds of CPU work per reference step")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world, local)
+    else:
+        run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,163 @@
+/*
+ * slcs.h -- C ABI of the B200 semi-local LCS engine (libslcs.so).
+ *
+ * Plain C types only (no CUDA or torch types): pointers, sizes, status codes.  Streams are passed as
+ * `void *` holding a cudaStream_t (NULL = the engine's own stream).  Every entry point returns an
+ * SLCS_* status; on failure slcs_last_error() gives a message for the calling thread.  Nothing here
+ * exits the process or falls back to the CPU: without a usable CUDA device every compute call returns
+ * SLCS_ERR_NO_DEVICE.
+ *
+ * Braid layout (identical to the reference's common::Permutation, R:common/include/Permutations/
+ * Matrices.h:16-96): a pair (a[0..m), b[0..n)) has m+n strands.  row_to_col[s] is the end of strand s:
+ *   strand starts (rows): left strands 0..m-1 (strand l enters the grid at row m-1-l),
+ *                         top strands m..m+n-1 (strand r enters at column r-m);
+ *   strand ends (cols):   bottom exits 0..n-1 (column j), right exits n..n+m-1 (n+l is row m-1-l).
+ * col_to_row is the inverse map.  Permutations for braid multiplication are n x n row->col maps.
+ *
+ * Reference interfaces replaced (paths relative to the reference project, R: = source/cpu/):
+ *   semi_local::SemiLocalStrategy<Input>::compute          R:include/SemiLocal/SemiLocalLCS.h:7-11
+ *   common::BraidMultiplicationStrategy::multiply           R:common/include/Permutations/MongeMultuplicationStrategy.h:18-21
+ *   common::StaggeredStickyBraidMultiplication::staggeredStickyMultiplication
+ *                                                           R:common/include/Permutations/MongeMultuplicationStrategy.h:679-758
+ *   lcs::LCSStrategy<Input>::compute                        R:include/LCS/LCS.h:9-13
+ *   prefix_lcs_via_semi_local::nary::llcs_nary_symbol_smart_combing
+ *                                                           R:prefix_lcs/bitwise/transposition_network_binary_alphabet.h:668-736
+ */
+#ifndef SLCS_H
+#define SLCS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------------- */
+#define SLCS_OK 0
+#define SLCS_ERR_ARG 1          /* invalid argument (negative size, NULL pointer, bad option) */
+#define SLCS_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define SLCS_ERR_OOM 3          /* device memory exhausted / admission budget exceeded */
+#define SLCS_ERR_TIMEOUT 4      /* a bounded device-side wait gave up (error word set by a kernel) */
+#define SLCS_ERR_TOO_LARGE 5    /* size beyond what the engine supports */
+#define SLCS_ERR_NO_DEVICE 6    /* no usable CUDA device */
+#define SLCS_ERR_INTERNAL 7     /* consistency check failed */
+#define SLCS_ERR_BUSY 8         /* server queue full / request not finished */
+
+/* ---- algorithm selection ------------------------------------------------------------------------ */
+#define SLCS_ALGO_AUTO 0        /* engine chooses (plain wavefront for small grids, hybrid above) */
+#define SLCS_ALGO_WAVEFRONT 1   /* tiled wavefront combing over the whole grid */
+#define SLCS_ALGO_HYBRID 2      /* tiles combed independently, glued by GPU steady ant */
+
+typedef struct slcs_opts {
+    int algo;            /* SLCS_ALGO_* */
+    int tile_rows;       /* hybrid tile height (0 = default 4096) */
+    int tile_cols;       /* hybrid tile width  (0 = default 4096) */
+    int band_rows;       /* wavefront rows per warp band: 32*R, R in {1,2,4,8,16,32} (0 = auto) */
+    int sa_cutoff;       /* steady-ant size below which sub-problems finish in shared memory (0 = default) */
+    int reserved[3];
+} slcs_opts;
+
+/* ---- library ------------------------------------------------------------------------------------ */
+int slcs_version(void);
+const char *slcs_last_error(void);
+/* Select the CUDA device used by the calling thread's engine calls (default 0). */
+int slcs_set_device(int device);
+/* Release cached device memory and engine state of the current device. */
+int slcs_release(void);
+
+/* ---- semi-local combing: the braid of a pair -------------------------------------------------- */
+/* Replaces semi_local::SemiLocalStrategy<Input>::compute (R:include/SemiLocal/SemiLocalLCS.h:7-11) for
+ * uint8 symbols; outputs row_to_col (m+n).  col_to_row and score (global LLCS) are optional (NULL).
+ * Host buffers; copies in and out are part of the call. */
+int slcs_comb_u8(const uint8_t *a, int m, const uint8_t *b, int n, int32_t *row_to_col, int32_t *col_to_row,
+                 int32_t *score, const slcs_opts *opts);
+/* Same for int32 symbols (Input = int in the reference); symbols are compared for equality only. */
+int slcs_comb_i32(const int32_t *a, int m, const int32_t *b, int n, int32_t *row_to_col, int32_t *col_to_row,
+                  int32_t *score, const slcs_opts *opts);
+/* Device-pointer variant: all pointers are device memory, work is ordered on `stream`. */
+int slcs_comb_u8_dev(const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_row_to_col,
+                     int32_t *d_col_to_row, int32_t *d_score, const slcs_opts *opts, void *stream);
+
+/* ---- global LCS score ------------------------------------------------------------------------- */
+/* Replaces lcs::LCSStrategy<Input>::compute (R:include/LCS/LCS.h:9-13) through the braid
+ * (lcs::LCSBySemiLocal, R:include/LCS/LCS.h:216-238). */
+int slcs_lcs_u8(const uint8_t *a, int m, const uint8_t *b, int n, int32_t *score);
+
+/* ---- bit-parallel combing (score only) -------------------------------------------------------- */
+/* LLCS by bit-parallel sticky-braid combing, one bit per strand; symbols must be < 4 (2-bit codes).
+ * Replaces prefix_lcs_via_semi_local::nary::llcs_nary_symbol_smart_combing with bits_per_symbol = 2
+ * (R:prefix_lcs/bitwise/transposition_network_binary_alphabet.h:668-736) and the binary variant
+ * (:598-663) for symbols < 2; unlike the reference any lengths are accepted. */
+int slcs_bitcomb_llcs_u8(const uint8_t *a, int m, const uint8_t *b, int n, int32_t *score);
+int slcs_bitcomb_llcs_u8_dev(const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_score, void *stream);
+
+/* ---- unit-Monge braid multiplication (steady ant) -------------------------------------------- */
+/* r = p (.) q for n x n permutations given as row->col maps.
+ * Replaces common::BraidMultiplicationStrategy::multiply
+ * (R:common/include/Permutations/MongeMultuplicationStrategy.h:18-21). */
+int slcs_steady_ant(const int32_t *p, const int32_t *q, int n, int32_t *r, const slcs_opts *opts);
+int slcs_steady_ant_dev(const int32_t *d_p, const int32_t *d_q, int n, int32_t *d_r, const slcs_opts *opts,
+                        void *stream);
+
+/* Glue braid p (pm rows of a, pn columns of b) with braid q sharing k strands.
+ * row_glue != 0: p above q (k = pn = qn); row_glue == 0: p left of q (k = pm = qm).
+ * Replaces common::StaggeredStickyBraidMultiplication::staggeredStickyMultiplication<RowGlue>
+ * (R:common/include/Permutations/MongeMultuplicationStrategy.h:679-758).  out has pm+pn+qm+qn-k entries. */
+int slcs_staggered_glue(const int32_t *p, int pm, int pn, const int32_t *q, int qm, int qn, int row_glue,
+                        int32_t *out);
+
+/* ---- scores read from a braid ----------------------------------------------------------------- */
+#define SLCS_Q_GLOBAL 0             /* LCS(a, b) */
+#define SLCS_Q_STRING_SUBSTRING 1   /* LCS(a, b[i..j)) */
+#define SLCS_Q_PREFIX_SUFFIX 2      /* LCS(a[0..i), b[j..n)) */
+#define SLCS_Q_SUFFIX_PREFIX 3      /* LCS(a[i..m), b[0..j)) */
+#define SLCS_Q_SUBSTRING_STRING 4   /* LCS(a[i..j), b) */
+#define SLCS_Q_MATRIX 5             /* raw semi-local matrix entry H(i, j), i, j in [0, m+n] */
+typedef struct slcs_query {
+    int32_t kind;
+    int32_t i;
+    int32_t j;
+} slcs_query;
+/* Answers nq queries against a braid (host row_to_col of m+n entries).  Semantics follow the
+ * semi-local matrix of R:include/SemiLocal/SemiLocalLCS.h:13-63 and the string-substring readout of
+ * R:approximate_matching/utils.h:281-334. */
+int slcs_scores(const int32_t *row_to_col, int m, int n, const slcs_query *q, int nq, int32_t *out);
+int slcs_scores_dev(const int32_t *d_row_to_col, int m, int n, const slcs_query *d_q, int nq, int32_t *d_out,
+                    void *stream);
+
+/* ---- batched combing -------------------------------------------------------------------------- */
+/* Braids of npairs independent pairs in one persistent, length-bucketed launch.  a_cat / b_cat hold the
+ * concatenated symbols, a_off / b_off (npairs) the start of each string, m / n (npairs) the lengths;
+ * row_to_col_cat receives the concatenated braids (pair i at offset sum_{j<i} m_j + n_j); scores
+ * (npairs, optional) the global LLCS.  The reference has no batch API: this replaces a loop of
+ * SemiLocalStrategy::compute calls.  mode 0 = persistent batched launch, 1 = one launch per pair. */
+int slcs_batch_comb_u8(const uint8_t *a_cat, const int64_t *a_off, const int32_t *m, const uint8_t *b_cat,
+                       const int64_t *b_off, const int32_t *n, int npairs, int32_t *row_to_col_cat,
+                       int32_t *scores, int mode, const slcs_opts *opts);
+
+/* ---- batch plans (device-resident batches, reusable, graph-capturable) ------------------------- */
+/* A plan fixes the pair lengths and owns the device buffers of one batch.  run() is the device-only
+ * step: one persistent length-bucketed launch (mode 0) or one launch per pair (mode 1), then the
+ * end->start inversion; with use_graph != 0 the step is captured once into a CUDA graph and replayed. */
+typedef struct slcs_batch slcs_batch;
+int slcs_batch_create(const int32_t *m, const int32_t *n, int npairs, int mode, const slcs_opts *opts,
+                      slcs_batch **out);
+int slcs_batch_upload(slcs_batch *bt, const uint8_t *a_cat, const int64_t *a_off, const uint8_t *b_cat,
+                      const int64_t *b_off, void *stream);
+int slcs_batch_run(slcs_batch *bt, int use_graph, void *stream);
+int slcs_batch_download(slcs_batch *bt, int32_t *row_to_col_cat, int32_t *scores, void *stream);
+/* Device time (ms) of the last run's combing kernel(s), measured with CUDA events on the run's stream. */
+int slcs_batch_kernel_ms(slcs_batch *bt, float *ms);
+/* Total cells (sum m*n) and launch count of one run. */
+int slcs_batch_info(slcs_batch *bt, int64_t *cells, int32_t *launches, int64_t *h2d_bytes, int64_t *d2h_bytes);
+int slcs_batch_destroy(slcs_batch *bt);
+
+/* ---- measurement helper (no counterpart in the reference) --------------------------------------- */
+/* Issue-rate ceiling of the combing cell's instruction mix on this device, in cells per second
+ * (independent cells at full occupancy): the denominator of the combing kernels' roofline fraction. */
+int slcs_probe_cell_peak(double *cells_per_sec);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SLCS_H */

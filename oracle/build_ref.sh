@@ -1,0 +1,24 @@
+#!/usr/bin/env bash
+# Compile the reference's own CPU headers (NikitaMishin/semilocal, source/cpu/) in place into
+# oracle/_ref/libslcs_ref.so through oracle/ref_shim.cpp.  TEST INFRASTRUCTURE ONLY: the library is the
+# parity pin for the C oracle, the generator of tests/golden/, and the "reference" CPU baseline of bench.py.
+#
+# The reference's CMake build is not used (its configure step needs GTest and a missing test file).
+# Only the header-only library code is compiled; nothing is copied out of the reference tree.
+#
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+set -euo pipefail
+here="$(cd "$(dirname "$0")" && pwd)"
+ref="${1:-/root/reference}"
+src="$ref/source/cpu"
+if [ ! -d "$src" ]; then
+  echo "build_ref: reference sources not found at $src; skipping" >&2
+  exit 0
+fi
+mkdir -p "$here/_ref"
+# -march=x86-64-v3: portable across the build container and the GPU hosts (the reference's own CMake uses
+# -march=native, which would tie the binary to this CPU).
+/usr/bin/g++ -std=c++17 -O3 -march=x86-64-v3 -fopenmp -fPIC -shared -w \
+  -I"$src" "$here/ref_shim.cpp" -o "$here/_ref/libslcs_ref.so.tmp" -Wl,--no-undefined
+mv "$here/_ref/libslcs_ref.so.tmp" "$here/_ref/libslcs_ref.so"
+echo "build_ref: wrote $here/_ref/libslcs_ref.so"

@@ -1,0 +1,324 @@
+"""ctypes face of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Two libraries are wrapped:
+  * liboracle.so   -- the C restatement in oracle/slcs_oracle.c (always built; `make -C oracle`);
+  * _ref/libslcs_ref.so -- the reference's own headers compiled by oracle/build_ref.sh (present when the
+    reference sources were available at build time; the file travels with the repository snapshot).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may import this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libslcs_ref.so")
+
+_lock = threading.Lock()
+_lib = None
+_ref = None
+_ref_tried = False
+
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+
+
+def build() -> str:
+    """(Re)build liboracle.so if it is missing or older than its source."""
+    src = os.path.join(HERE, "slcs_oracle.c")
+    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-C", HERE, "-s"], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    with _lock:
+        if _lib is None:
+            build()
+            L = ctypes.CDLL(LIB_PATH)
+            L.slo_comb_rowmajor.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, _i32p]
+            L.slo_comb_antidiag.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int, _i32p]
+            L.slo_rotate180.argtypes = [_i32p, ctypes.c_int, _i32p]
+            L.slo_semilocal_matrix.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, _i32p]
+            L.slo_kernel_from_matrix.argtypes = [_i32p, ctypes.c_int, ctypes.c_int, _i32p]
+            L.slo_global_score.argtypes = [_i32p, ctypes.c_int, ctypes.c_int]
+            L.slo_semilocal_entry.argtypes = [_i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+            L.slo_lcs_dp.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int]
+            L.slo_braid_mult_naive.argtypes = [_i32p, _i32p, ctypes.c_int, _i32p]
+            L.slo_steady_ant.argtypes = [_i32p, _i32p, ctypes.c_int, _i32p]
+            L.slo_staggered.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i32p]
+            L.slo_hybrid_iterative.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_int, _i32p]
+            L.slo_encode_u64.argtypes = [_i32p, ctypes.c_int, ctypes.c_int, _u64p]
+            L.slo_encode_reverse_u64.argtypes = [_i32p, ctypes.c_int, ctypes.c_int, _u64p]
+            L.slo_bit_llcs_nary_u64.argtypes = [_u64p, ctypes.c_int, _u64p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+            L.slo_bit_llcs_binary_u64.argtypes = [_u64p, ctypes.c_int, _u64p, ctypes.c_int, ctypes.c_int]
+            L.slo_comb_score.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int]
+            _lib = L
+    return _lib
+
+
+def ref():
+    """The reference-compiled library, or None when it was not built."""
+    global _ref, _ref_tried
+    with _lock:
+        if not _ref_tried:
+            _ref_tried = True
+            if os.path.exists(REF_PATH):
+                R = ctypes.CDLL(REF_PATH)
+                R.ref_comb_simple.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, _i32p]
+                R.ref_comb_openmp.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int, _i32p]
+                R.ref_comb_dummy.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, _i32p]
+                R.ref_comb_combined.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int, _i32p]
+                R.ref_hybrid_iterative.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int,
+                                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, _i32p]
+                R.ref_hybrid_recursive.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int,
+                                                   ctypes.c_int, ctypes.c_int, _i32p]
+                R.ref_braid_naive.argtypes = [_i32p, _i32p, ctypes.c_int, _i32p]
+                R.ref_braid_simple.argtypes = [_i32p, _i32p, ctypes.c_int, ctypes.c_int, _i32p]
+                R.ref_braid_seq.argtypes = [_i32p, _i32p, ctypes.c_int, ctypes.c_int, _i32p]
+                R.ref_braid_omp.argtypes = [_i32p, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i32p]
+                R.ref_precalc_warm.argtypes = [ctypes.c_int]
+                R.ref_staggered.argtypes = [_i32p, ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, _i32p]
+                R.ref_lcs_seqmem.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int]
+                R.ref_lcs_dummy.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int]
+                R.ref_lcs_by_semilocal.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int]
+                R.ref_bit_nary_u64.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+                R.ref_bit_binary_u64.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int]
+                _ref = R
+    return _ref
+
+
+def _i32(x) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x, dtype=np.int32))
+
+
+def _p(x: np.ndarray):
+    return x.ctypes.data_as(_i32p)
+
+
+def _pu(x: np.ndarray):
+    return x.ctypes.data_as(_u64p)
+
+
+# --------------------------------------------------------------------------------------------------
+# C restatement
+# --------------------------------------------------------------------------------------------------
+
+def comb_rowmajor(a, b) -> np.ndarray:
+    a, b = _i32(a), _i32(b)
+    out = np.empty(len(a) + len(b), dtype=np.int32)
+    lib().slo_comb_rowmajor(_p(a), len(a), _p(b), len(b), _p(out))
+    return out
+
+
+def comb_antidiag(a, b, threads: int = 1) -> np.ndarray:
+    a, b = _i32(a), _i32(b)
+    out = np.empty(len(a) + len(b), dtype=np.int32)
+    lib().slo_comb_antidiag(_p(a), len(a), _p(b), len(b), threads, _p(out))
+    return out
+
+
+def rotate180(perm) -> np.ndarray:
+    perm = _i32(perm)
+    out = np.full(len(perm), -1, dtype=np.int32)
+    lib().slo_rotate180(_p(perm), len(perm), _p(out))
+    return out
+
+
+def semilocal_matrix(a, b) -> np.ndarray:
+    a, b = _i32(a), _i32(b)
+    s = len(a) + len(b) + 1
+    H = np.empty(s * s, dtype=np.int32)
+    lib().slo_semilocal_matrix(_p(a), len(a), _p(b), len(b), _p(H))
+    return H.reshape(s, s)
+
+
+def kernel_from_matrix(H, m: int, n: int) -> np.ndarray:
+    H = _i32(H).ravel()
+    out = np.empty(m + n, dtype=np.int32)
+    lib().slo_kernel_from_matrix(_p(H), m, n, _p(out))
+    return out
+
+
+def comb_dp(a, b) -> np.ndarray:
+    """Braid from the DP definition of the semi-local matrix (small sizes only)."""
+    return kernel_from_matrix(semilocal_matrix(a, b), len(a), len(b))
+
+
+def global_score(perm, m: int, n: int) -> int:
+    perm = _i32(perm)
+    return int(lib().slo_global_score(_p(perm), m, n))
+
+
+def semilocal_entry(perm, m: int, n: int, i: int, j: int) -> int:
+    perm = _i32(perm)
+    return int(lib().slo_semilocal_entry(_p(perm), m, n, i, j))
+
+
+def lcs_dp(a, b) -> int:
+    a, b = _i32(a), _i32(b)
+    return int(lib().slo_lcs_dp(_p(a), len(a), _p(b), len(b)))
+
+
+def braid_naive(p, q) -> np.ndarray:
+    p, q = _i32(p), _i32(q)
+    out = np.empty(len(p), dtype=np.int32)
+    lib().slo_braid_mult_naive(_p(p), _p(q), len(p), _p(out))
+    return out
+
+
+def steady_ant(p, q) -> np.ndarray:
+    p, q = _i32(p), _i32(q)
+    out = np.empty(len(p), dtype=np.int32)
+    rc = lib().slo_steady_ant(_p(p), _p(q), len(p), _p(out))
+    if rc != 0:
+        raise RuntimeError("oracle steady ant failed")
+    return out
+
+
+def staggered(p, pm: int, pn: int, q, qm: int, qn: int, row_glue: bool) -> np.ndarray:
+    p, q = _i32(p), _i32(q)
+    k = pn if row_glue else pm
+    out = np.empty(pm + pn + qm + qn - k, dtype=np.int32)
+    rc = lib().slo_staggered(_p(p), pm + pn, _p(q), qm + qn, k, int(bool(row_glue)), _p(out))
+    if rc != 0:
+        raise RuntimeError("oracle staggered glue failed")
+    return out
+
+
+def hybrid_iterative(a, b, threads: int = 1, cols: int = 4096, rows: int = 4096) -> np.ndarray:
+    a, b = _i32(a), _i32(b)
+    out = np.empty(len(a) + len(b), dtype=np.int32)
+    rc = lib().slo_hybrid_iterative(_p(a), len(a), _p(b), len(b), threads, cols, rows, _p(out))
+    if rc != 0:
+        raise RuntimeError("oracle hybrid failed")
+    return out
+
+
+def encode_u64(s, bps: int) -> np.ndarray:
+    s = _i32(s)
+    S = 64 // bps
+    out = np.zeros(max(1, (len(s) + S - 1) // S), dtype=np.uint64)
+    w = lib().slo_encode_u64(_p(s), len(s), bps, _pu(out))
+    return out[:w]
+
+
+def encode_reverse_u64(s, bps: int) -> np.ndarray:
+    s = _i32(s)
+    S = 64 // bps
+    out = np.zeros(max(1, (len(s) + S - 1) // S), dtype=np.uint64)
+    w = lib().slo_encode_reverse_u64(_p(s), len(s), bps, _pu(out))
+    return out[:w]
+
+
+def bit_llcs_nary(a, b, bps: int = 2) -> int:
+    """Reference-domain n-ary bit combing (lengths multiples of 64/bps, |a| <= |b|)."""
+    ar = encode_reverse_u64(a, bps)
+    be = encode_u64(b, bps)
+    return int(lib().slo_bit_llcs_nary_u64(_pu(ar), len(ar), _pu(be), len(be), len(a), bps))
+
+
+def bit_llcs_binary(a, b) -> int:
+    ar = encode_reverse_u64(a, 1)
+    be = encode_u64(b, 1)
+    return int(lib().slo_bit_llcs_binary_u64(_pu(ar), len(ar), _pu(be), len(be), len(a)))
+
+
+def comb_score(a, b, threads: int = 1) -> int:
+    a, b = _i32(a), _i32(b)
+    return int(lib().slo_comb_score(_p(a), len(a), _p(b), len(b), threads))
+
+
+# --------------------------------------------------------------------------------------------------
+# Reference-compiled checker (None-returning when absent)
+# --------------------------------------------------------------------------------------------------
+
+def ref_available() -> bool:
+    return ref() is not None
+
+
+def ref_comb(a, b, kind: str = "simple", threads: int = 1) -> np.ndarray:
+    R = ref()
+    a, b = _i32(a), _i32(b)
+    out = np.empty(len(a) + len(b), dtype=np.int32)
+    if kind == "simple":
+        R.ref_comb_simple(_p(a), len(a), _p(b), len(b), _p(out))
+    elif kind == "openmp":
+        R.ref_comb_openmp(_p(a), len(a), _p(b), len(b), threads, _p(out))
+    elif kind == "dummy":
+        R.ref_comb_dummy(_p(a), len(a), _p(b), len(b), _p(out))
+    elif kind == "combined":
+        R.ref_comb_combined(_p(a), len(a), _p(b), len(b), threads, _p(out))
+    else:
+        raise ValueError(kind)
+    return out
+
+
+def ref_hybrid_iterative(a, b, threads=1, cols=4096, rows=4096, precalc=0) -> np.ndarray:
+    R = ref()
+    a, b = _i32(a), _i32(b)
+    out = np.empty(len(a) + len(b), dtype=np.int32)
+    R.ref_hybrid_iterative(_p(a), len(a), _p(b), len(b), threads, cols, rows, precalc, _p(out))
+    return out
+
+
+def ref_hybrid_recursive(a, b, parallel_depth=1, depth=6, sum_bound=400) -> np.ndarray:
+    R = ref()
+    a, b = _i32(a), _i32(b)
+    out = np.empty(len(a) + len(b), dtype=np.int32)
+    R.ref_hybrid_recursive(_p(a), len(a), _p(b), len(b), parallel_depth, depth, sum_bound, _p(out))
+    return out
+
+
+def ref_braid(p, q, kind: str = "seq", precalc: int = 0, depth: int = 3) -> np.ndarray:
+    R = ref()
+    p, q = _i32(p), _i32(q)
+    out = np.empty(len(p), dtype=np.int32)
+    if kind == "naive":
+        R.ref_braid_naive(_p(p), _p(q), len(p), _p(out))
+    elif kind == "simple":
+        R.ref_braid_simple(_p(p), _p(q), len(p), precalc, _p(out))
+    elif kind == "seq":
+        R.ref_braid_seq(_p(p), _p(q), len(p), precalc, _p(out))
+    elif kind == "omp":
+        R.ref_braid_omp(_p(p), _p(q), len(p), depth, precalc, _p(out))
+    else:
+        raise ValueError(kind)
+    return out
+
+
+def ref_staggered(p, pm, pn, q, qm, qn, row_glue: bool) -> np.ndarray:
+    R = ref()
+    p, q = _i32(p), _i32(q)
+    k = pn if row_glue else pm
+    out = np.empty(pm + pn + qm + qn - k, dtype=np.int32)
+    R.ref_staggered(_p(p), pm, pn, _p(q), qm, qn, int(bool(row_glue)), _p(out))
+    return out
+
+
+def ref_lcs(a, b, kind: str = "seqmem") -> int:
+    R = ref()
+    a, b = _i32(a), _i32(b)
+    f = {"seqmem": R.ref_lcs_seqmem, "dummy": R.ref_lcs_dummy, "semilocal": R.ref_lcs_by_semilocal}[kind]
+    return int(f(_p(a), len(a), _p(b), len(b)))
+
+
+def ref_bit_nary(a, b, alphabet: int = 4, threads: int = 1) -> int:
+    R = ref()
+    a, b = _i32(a), _i32(b)
+    return int(R.ref_bit_nary_u64(_p(a), len(a), _p(b), len(b), alphabet, threads))
+
+
+def ref_bit_binary(a, b, threads: int = 1) -> int:
+    R = ref()
+    a, b = _i32(a), _i32(b)
+    return int(R.ref_bit_binary_u64(_p(a), len(a), _p(b), len(b), threads))

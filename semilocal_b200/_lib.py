@@ -1,0 +1,122 @@
+"""Loader of libslcs.so (the CUDA engine) and ctypes signatures of its C ABI (include/slcs.h).
+
+The library is built in-tree for sm_100a by semilocal_b200/build.py.  There is no CPU fallback: if the
+library cannot be loaded, or the device is not usable, every call raises SlcsError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libslcs.so")
+
+SLCS_OK = 0
+ERRORS = {
+    1: "SLCS_ERR_ARG", 2: "SLCS_ERR_CUDA", 3: "SLCS_ERR_OOM", 4: "SLCS_ERR_TIMEOUT", 5: "SLCS_ERR_TOO_LARGE",
+    6: "SLCS_ERR_NO_DEVICE", 7: "SLCS_ERR_INTERNAL", 8: "SLCS_ERR_BUSY",
+}
+
+ALGO_AUTO, ALGO_WAVEFRONT, ALGO_HYBRID = 0, 1, 2
+Q_GLOBAL, Q_STRING_SUBSTRING, Q_PREFIX_SUFFIX, Q_SUFFIX_PREFIX, Q_SUBSTRING_STRING, Q_MATRIX = range(6)
+
+
+class SlcsError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("algo", ctypes.c_int), ("tile_rows", ctypes.c_int), ("tile_cols", ctypes.c_int),
+                ("band_rows", ctypes.c_int), ("sa_cutoff", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
+
+
+class Query(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("i", ctypes.c_int32), ("j", ctypes.c_int32)]
+
+
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_vp = ctypes.c_void_p
+_int = ctypes.c_int
+_optp = ctypes.POINTER(Opts)
+_qp = ctypes.POINTER(Query)
+
+# name -> argtypes (all return int status except where noted)
+SIGNATURES = {
+    "slcs_version": [],
+    "slcs_set_device": [_int],
+    "slcs_release": [],
+    "slcs_comb_u8": [_u8p, _int, _u8p, _int, _i32p, _i32p, _i32p, _optp],
+    "slcs_comb_i32": [_i32p, _int, _i32p, _int, _i32p, _i32p, _i32p, _optp],
+    "slcs_comb_u8_dev": [_vp, _int, _vp, _int, _vp, _vp, _vp, _optp, _vp],
+    "slcs_lcs_u8": [_u8p, _int, _u8p, _int, _i32p],
+    "slcs_bitcomb_llcs_u8": [_u8p, _int, _u8p, _int, _i32p],
+    "slcs_bitcomb_llcs_u8_dev": [_vp, _int, _vp, _int, _vp, _vp],
+    "slcs_steady_ant": [_i32p, _i32p, _int, _i32p, _optp],
+    "slcs_steady_ant_dev": [_vp, _vp, _int, _vp, _optp, _vp],
+    "slcs_staggered_glue": [_i32p, _int, _int, _i32p, _int, _int, _int, _i32p],
+    "slcs_scores": [_i32p, _int, _int, _qp, _int, _i32p],
+    "slcs_scores_dev": [_vp, _int, _int, _vp, _int, _vp, _vp],
+    "slcs_batch_comb_u8": [_u8p, _i64p, _i32p, _u8p, _i64p, _i32p, _int, _i32p, _i32p, _int, _optp],
+    "slcs_batch_create": [_i32p, _i32p, _int, _int, _optp, ctypes.POINTER(_vp)],
+    "slcs_batch_upload": [_vp, _vp, _i64p, _vp, _i64p, _vp],
+    "slcs_batch_run": [_vp, _int, _vp],
+    "slcs_batch_download": [_vp, _vp, _vp, _vp],
+    "slcs_batch_kernel_ms": [_vp, ctypes.POINTER(ctypes.c_float)],
+    "slcs_batch_info": [_vp, _i64p, _i32p, _i64p, _i64p],
+    "slcs_batch_destroy": [_vp],
+    "slcs_probe_cell_peak": [ctypes.POINTER(ctypes.c_double)],
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def _ensure_built() -> None:
+    if os.path.exists(LIB_PATH):
+        from . import build as _b
+        if not _b.stale():
+            return
+        try:
+            _b.build()
+        except Exception:
+            # a stale but present library still works; a rebuild failure is reported on the next build()
+            return
+        return
+    from . import build as _b
+    _b.build()
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded engine library (built on first use when nvcc is available)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            _ensure_built()
+            if not os.path.exists(LIB_PATH):
+                raise SlcsError(6, f"libslcs.so not found at {LIB_PATH}; run semilocal_b200/build.py")
+            L = ctypes.CDLL(LIB_PATH)
+            for name, args in SIGNATURES.items():
+                fn = getattr(L, name)
+                fn.argtypes = args
+                fn.restype = ctypes.c_int
+            L.slcs_last_error.argtypes = []
+            L.slcs_last_error.restype = ctypes.c_char_p
+            _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != SLCS_OK:
+        msg = lib().slcs_last_error()
+        raise SlcsError(rc, msg.decode(errors="replace") if msg else "")
+
+
+def opts(algo: int = ALGO_AUTO, tile_rows: int = 0, tile_cols: int = 0, band_rows: int = 0, sa_cutoff: int = 0):
+    o = Opts()
+    o.algo, o.tile_rows, o.tile_cols, o.band_rows, o.sa_cutoff = algo, tile_rows, tile_cols, band_rows, sa_cutoff
+    return o

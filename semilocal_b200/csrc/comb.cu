@@ -1,0 +1,204 @@
+// comb.cu -- integer sticky-braid combing on sm_100a.
+//
+// The grid of a pair (rows = symbols of a, columns = symbols of b) is cut into horizontal bands of 32*R rows.
+// One warp combs one band: lane l owns R consecutive rows (their left strands and a-symbols stay in
+// registers for the whole band) and the warp is a 32-stage systolic array: at step s lane l processes
+// column s - l, the strand leaving a lane's last row goes down to the next lane by a warp shuffle.
+// The warp exchanges 32 columns at a time with the band above / below through the pair's output array
+// (entries 0..n-1 hold the top strands handed down band by band, in place), synchronised by a per-band
+// progress counter (release/acquire, bounded spins that give up into the device error word).
+// Work items (pair, band) are dequeued in order by persistent warps, so a band only ever waits for a band
+// that an already-running warp owns: no co-residency assumption, no deadlock.
+//
+// Cell rule (R:include/SemiLocal/SemiLocalLCS.h:153-174, canonical form :81-114): the strands swap iff the
+// symbols match or the left strand's id is larger than the top strand's.
+// Output (ends -> starts, R:include/SemiLocal/SemiLocalLCS.h:117-121): column j < n receives the strand
+// leaving the bottom of column j, column n+l the strand leaving the right side of row m-1-l.
+#include "slcs_internal.cuh"
+
+namespace slcs {
+namespace {
+
+constexpr int kSymRowVirtual = -0x40000000;   // a-symbol of a padding row: matches nothing
+constexpr int kSymColVirtual = -0x40000001;   // b-symbol of a padding column: matches nothing
+constexpr int kStrandPad = 0x7fffffff;        // strand of a padding column: never smaller than a left strand
+
+template <typename T, int R>
+__device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, int *err, int lane) {
+    const T *__restrict__ a = static_cast<const T *>(P.a);
+    const T *__restrict__ b = static_cast<const T *>(P.b);
+    const int m = P.m, n = P.n;
+    const int rbase = I.r0 + lane * R;
+
+    int A[R], L[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int row = rbase + k;
+        if (row < m) {
+            A[k] = static_cast<int>(a[row]);
+            L[k] = m - 1 - row;
+        } else {
+            A[k] = kSymRowVirtual;
+            L[k] = -1;
+        }
+    }
+
+    const bool has_prev = I.band > 0;
+    const int *prev_prog = has_prev ? P.progress + (I.band - 1) : nullptr;
+    int *my_prog = P.progress + I.band;
+    const int nchunks = (n + 63) >> 5;   // steps 0 .. n+31 (column n-1 leaves the warp at step n+31)
+
+    int io_t = kStrandPad, io_b = kSymColVirtual;
+    // Loads the top strands and b-symbols of columns [32q, 32q+32) into io (lane j <- column 32q+j).
+    auto load = [&](int q) -> bool {
+        const int c0 = q << 5;
+        if (has_prev && c0 < n) {
+            int ok = 1;
+            if (lane == 0) ok = wait_at_least(prev_prog, min(n, c0 + 32), err) ? 1 : 0;
+            ok = __shfl_sync(kFull, ok, 0);
+            if (!ok) return false;
+        }
+        const int c = c0 + lane;
+        if (c < n) {
+            io_t = has_prev ? __ldcg(P.c2r + c) : (m + c);
+            io_b = static_cast<int>(b[c]);
+        } else {
+            io_t = kStrandPad;
+            io_b = kSymColVirtual;
+        }
+        return true;
+    };
+
+    if (!load(0)) return;
+    int t = kStrandPad, bs = kSymColVirtual;
+    const int src_dn = (lane + 31) & 31, src_up = (lane + 1) & 31;
+    for (int q = 0; q < nchunks; ++q) {
+#pragma unroll 4
+        for (int k = 0; k < 32; ++k) {
+            // systolic shift: lane l takes the strand (and symbol) lane l-1 produced one step ago;
+            // lane 0 receives the warp's bottom output instead, parks it in io and takes the next input.
+            t = __shfl_sync(kFull, t, src_dn);
+            bs = __shfl_sync(kFull, bs, src_dn);
+            if (lane == 0) {
+                const int x = t;
+                t = io_t;
+                io_t = x;
+                bs = io_b;
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const bool sw = (A[r] == bs) | (L[r] > t);
+                const int nt = sw ? L[r] : t;
+                L[r] = sw ? t : L[r];
+                t = nt;
+            }
+            io_t = __shfl_sync(kFull, io_t, src_up);
+            io_b = __shfl_sync(kFull, io_b, src_up);
+        }
+        // io_t of lane j now holds the strand that left the band's bottom in column 32(q-1)+j.
+        const int col = ((q - 1) << 5) + lane;
+        const bool valid = col >= 0 && col < n;
+        if (valid) __stcg(P.c2r + col, io_t);
+        if (I.last && P.score != nullptr) {
+            const unsigned bal = __ballot_sync(kFull, valid && io_t < m);
+            if (lane == 0 && bal) atomicAdd(P.score, __popc(bal));
+        }
+        __syncwarp();
+        if (!I.last && lane == 0) st_release(my_prog, min(n, q << 5));
+        if (q + 1 < nchunks && !load(q + 1)) return;
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int row = rbase + k;
+        if (row < m) P.c2r[n + (m - 1 - row)] = L[k];
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128, 3) comb_kernel(const CombPair *__restrict__ pairs,
+                                                   const CombItem *__restrict__ items, int nitems, int *next,
+                                                   int *err) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int it = nitems;
+        if (lane == 0 && ld_relaxed(err) == kDevErrNone) it = atomicAdd(next, 1);
+        it = __shfl_sync(kFull, it, 0);
+        if (it >= nitems) return;
+        const CombItem I = items[it];
+        const CombPair P = pairs[I.pair];
+        switch (I.R) {
+            case 32: comb_band<T, 32>(P, I, err, lane); break;
+            case 16: comb_band<T, 16>(P, I, err, lane); break;
+            case 8: comb_band<T, 8>(P, I, err, lane); break;
+            case 4: comb_band<T, 4>(P, I, err, lane); break;
+            case 2: comb_band<T, 2>(P, I, err, lane); break;
+            default: comb_band<T, 1>(P, I, err, lane); break;
+        }
+    }
+}
+
+__global__ void invert_kernel(const int32_t *__restrict__ c2r, int size, int32_t *__restrict__ r2c, int rot) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < size; i += gridDim.x * blockDim.x) {
+        const int r = c2r[i];
+        if (rot) r2c[size - 1 - r] = size - 1 - i;
+        else r2c[r] = i;
+    }
+}
+
+}  // namespace
+
+int plan_bands(int pair, int m, int R, std::vector<CombItem> &items) {
+    int Rmax = 1;
+    while (Rmax * 2 <= R && Rmax < 32) Rmax *= 2;
+    const size_t first = items.size();
+    int r0 = 0, band = 0;
+    while (r0 < m) {
+        const int rem = m - r0;
+        // smallest band height covering the rest; taken when it pads by at most a third
+        int Rc = 1;
+        while (32 * Rc < rem) Rc *= 2;
+        if (Rc <= Rmax && (3 * 32 * Rc <= 4 * rem || rem <= 32)) {
+            items.push_back(CombItem{pair, band++, r0, Rc, 0});
+            break;
+        }
+        // otherwise the largest band height the rest fills completely
+        int Rf = 1;
+        while (Rf * 2 <= Rmax && 32 * Rf * 2 <= rem) Rf *= 2;
+        items.push_back(CombItem{pair, band++, r0, Rf, 0});
+        r0 += 32 * Rf;
+    }
+    if (items.size() > first) items.back().last = 1;
+    return band;
+}
+
+template <typename T>
+int launch_comb(const CombPair *d_pairs, const CombItem *d_items, int nitems, int *d_next, int *d_err,
+                int grid_warps, cudaStream_t s) {
+    if (nitems <= 0) return SLCS_OK;
+    const int warps = grid_warps < nitems ? grid_warps : nitems;
+    const int blocks = (warps + 3) / 4;
+    comb_kernel<T><<<blocks, 128, 0, s>>>(d_pairs, d_items, nitems, d_next, d_err);
+    SLCS_CUDA_TRY(cudaGetLastError());
+    return SLCS_OK;
+}
+template int launch_comb<uint8_t>(const CombPair *, const CombItem *, int, int *, int *, int, cudaStream_t);
+template int launch_comb<int32_t>(const CombPair *, const CombItem *, int, int *, int *, int, cudaStream_t);
+
+int comb_resident_warps(Engine *E) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, comb_kernel<uint8_t>, 128, 0) != cudaSuccess ||
+        per_sm <= 0)
+        per_sm = 4;
+    return per_sm * 4 * E->num_sms;
+}
+
+int launch_invert(const int32_t *c2r, int size, int32_t *r2c, bool rot180, cudaStream_t s) {
+    if (size <= 0) return SLCS_OK;
+    int blocks = (size + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    invert_kernel<<<blocks, 256, 0, s>>>(c2r, size, r2c, rot180 ? 1 : 0);
+    SLCS_CUDA_TRY(cudaGetLastError());
+    return SLCS_OK;
+}
+
+}  // namespace slcs

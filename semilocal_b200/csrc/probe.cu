@@ -1,0 +1,74 @@
+// probe.cu -- measured ceiling of the combing cell's instruction mix (the integer-pipe roofline).
+//
+// Every thread runs 8 independent combing cells per iteration (distinct a-symbols, independent strand
+// pairs), i.e. the cell rule of comb.cu without its data dependencies, shuffles or memory traffic.  The
+// resulting cells/s, at full occupancy, is the issue-rate ceiling that the combing kernels are measured
+// against ("roofline.peak"); 5 integer ops per cell is the reporting convention (compare, compare, or,
+// two selects).
+#include "slcs_internal.cuh"
+
+namespace slcs {
+namespace {
+
+__global__ void __launch_bounds__(256) probe_cells_kernel(int iters, int seed, int *out) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    int L[8], t[8], A[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        L[k] = tid * 8 + k + seed;
+        t[k] = tid * 8 + 7 - k;
+        A[k] = (tid + k + seed) & 3;
+    }
+    int bs = (blockIdx.x + seed) & 3;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const bool sw = (A[k] == bs) | (L[k] > t[k]);
+            const int nt = sw ? L[k] : t[k];
+            L[k] = sw ? t[k] : L[k];
+            t[k] = nt;
+        }
+        bs = t[i & 7] & 3;
+    }
+    int acc = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc ^= L[k] + t[k];
+    if (acc == 0x12345678) out[0] = acc;   // keeps the work observable
+}
+
+}  // namespace
+}  // namespace slcs
+
+using namespace slcs;
+
+extern "C" int slcs_probe_cell_peak(double *cells_per_sec) {
+    if (!cells_per_sec) return fail(SLCS_ERR_ARG, "NULL output");
+    Engine *E;
+    SLCS_TRY(engine(&E));
+    cudaStream_t s = E->stream;
+    DevBuf<int> out;
+    SLCS_TRY(out.alloc(1, s));
+    int per_sm = 0;
+    SLCS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, probe_cells_kernel, 256, 0));
+    const int blocks = per_sm * E->num_sms;
+    const int iters = 4096;
+    cudaEvent_t e0, e1;
+    SLCS_CUDA_TRY(cudaEventCreate(&e0));
+    SLCS_CUDA_TRY(cudaEventCreate(&e1));
+    probe_cells_kernel<<<blocks, 256, 0, s>>>(iters, 1, out.p);   // warm-up
+    float best = 1e30f;
+    for (int rep = 0; rep < 5; ++rep) {
+        SLCS_CUDA_TRY(cudaEventRecord(e0, s));
+        probe_cells_kernel<<<blocks, 256, 0, s>>>(iters, rep, out.p);
+        SLCS_CUDA_TRY(cudaEventRecord(e1, s));
+        SLCS_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0;
+        SLCS_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) best = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double cells = (double) blocks * 256 * iters * 8;
+    *cells_per_sec = cells / (best * 1e-3);
+    return SLCS_OK;
+}

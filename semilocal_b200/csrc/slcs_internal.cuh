@@ -1,0 +1,145 @@
+// slcs_internal.cuh -- shared helpers of the B200 semi-local LCS engine (not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda/atomic>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/slcs.h"
+
+namespace slcs {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWarp = 32;
+
+// Device-side error word values (the first failing kernel wins; the host maps them to SLCS_ERR_*).
+constexpr int kDevErrNone = 0;
+constexpr int kDevErrTimeout = 1;     // a bounded spin gave up
+constexpr int kDevErrBadState = 2;    // an internal consistency check failed
+
+// Spin limits: each wait gives up after kSpinLimit polls (sleeping ~kSpinSleepNs between polls), i.e.
+// after a few seconds, sets the error word and returns; waiters also leave as soon as the word is set.
+constexpr long long kSpinLimit = 1ll << 25;
+constexpr unsigned kSpinSleepNs = 100;
+
+// ------------------------------------------------------------------------------------------------
+// host error plumbing
+// ------------------------------------------------------------------------------------------------
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+
+#define SLCS_CUDA_TRY(expr)                                                                          \
+    do {                                                                                             \
+        cudaError_t _e = (expr);                                                                     \
+        if (_e != cudaSuccess) {                                                                     \
+            return ::slcs::fail(_e == cudaErrorMemoryAllocation ? SLCS_ERR_OOM : SLCS_ERR_CUDA,      \
+                                std::string(#expr) + ": " + cudaGetErrorString(_e));                 \
+        }                                                                                            \
+    } while (0)
+
+#define SLCS_TRY(expr)                    \
+    do {                                  \
+        int _rc = (expr);                 \
+        if (_rc != SLCS_OK) return _rc;   \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------------
+// device helpers
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    cuda::atomic_ref<int, cuda::thread_scope_device> r(*const_cast<int *>(p));
+    return r.load(cuda::memory_order_acquire);
+}
+__device__ __forceinline__ void st_release(int *p, int v) {
+    cuda::atomic_ref<int, cuda::thread_scope_device> r(*p);
+    r.store(v, cuda::memory_order_release);
+}
+__device__ __forceinline__ int ld_relaxed(const int *p) {
+    cuda::atomic_ref<int, cuda::thread_scope_device> r(*const_cast<int *>(p));
+    return r.load(cuda::memory_order_relaxed);
+}
+__device__ __forceinline__ void raise_error(int *err, int code) { atomicCAS(err, kDevErrNone, code); }
+
+// Wait until *p >= need.  Returns false (after setting *err) when the bounded spin gives up or when
+// another thread already reported an error.  Called by one lane; the caller broadcasts the outcome.
+__device__ __forceinline__ bool wait_at_least(const int *p, int need, int *err) {
+    if (ld_acquire(p) >= need) return true;
+    for (long long it = 0; it < kSpinLimit; ++it) {
+        __nanosleep(kSpinSleepNs);
+        if (ld_acquire(p) >= need) return true;
+        if (ld_relaxed(err) != kDevErrNone) return false;
+    }
+    raise_error(err, kDevErrTimeout);
+    return false;
+}
+
+// ------------------------------------------------------------------------------------------------
+// per-device engine state: stream, error word, scratch arena
+// ------------------------------------------------------------------------------------------------
+struct Engine {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    bool ready = false;
+};
+
+// Returns the calling thread's engine for its current device, initialising it on first use.
+int engine(Engine **out);
+// Stream-ordered scratch allocation (cudaMallocAsync on the engine's memory pool).
+int dalloc(void **p, size_t bytes, cudaStream_t s);
+void dfree(void *p, cudaStream_t s);
+// Waits for the stream, then maps the device error word to an SLCS_* status.
+int check_dev_err(const int *d_err, cudaStream_t s);
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    cudaStream_t s = nullptr;
+    size_t count = 0;
+    int alloc(size_t cnt, cudaStream_t st) {
+        s = st;
+        count = cnt;
+        return dalloc(reinterpret_cast<void **>(&p), (cnt ? cnt : 1) * sizeof(T), st);
+    }
+    ~DevBuf() {
+        if (p) dfree(p, s);
+    }
+};
+
+// ------------------------------------------------------------------------------------------------
+// combing (comb.cu)
+// ------------------------------------------------------------------------------------------------
+struct CombPair {
+    const void *a;        // symbols of the row string (T)
+    const void *b;        // symbols of the column string (T)
+    int32_t *c2r;         // out: strand end -> strand start (m+n); also the band-to-band hand-off of the
+                          //      top strands (entries 0..n-1)
+    int32_t *progress;    // per band: number of leading columns whose hand-off value is final
+    int32_t *score;       // out (optional): global LLCS
+    int m, n;
+};
+
+struct CombItem {
+    int pair;
+    int band;    // band index inside the pair
+    int r0;      // first row of the band
+    int R;       // rows per lane (band height 32 R), in {1, 2, 4, 8, 16, 32}
+    int last;    // 1 if this is the pair's last band (its bottom outputs are final)
+};
+
+// Plans the bands of one pair: appends items with the given default R (the last band uses the smallest
+// R that still covers its rows).  Returns the number of bands.
+int plan_bands(int pair, int m, int R, std::vector<CombItem> &items);
+// Launch the persistent combing kernel over items (device arrays).  T = uint8_t or int32_t.
+template <typename T>
+int launch_comb(const CombPair *d_pairs, const CombItem *d_items, int nitems, int *d_next, int *d_err,
+                int grid_warps, cudaStream_t s);
+// Warps that fit on the device at once for the combing kernel.
+int comb_resident_warps(Engine *E);
+// c2r -> r2c for one pair (optionally rotated by 180 degrees), and the batched version.
+int launch_invert(const int32_t *c2r, int size, int32_t *r2c, bool rot180, cudaStream_t s);
+
+}  // namespace slcs
