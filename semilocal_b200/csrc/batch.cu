@@ -14,11 +14,18 @@ namespace slcs {
 namespace {
 
 __global__ void invert_batch_kernel(const int32_t *__restrict__ c2r_cat, const int64_t *__restrict__ out_off,
-                                    int32_t *__restrict__ r2c_cat) {
+                                    int32_t *__restrict__ r2c_cat, int *err) {
     const int p = blockIdx.x;
     const int64_t o = out_off[p];
     const int size = (int) (out_off[p + 1] - o);
-    for (int i = threadIdx.x; i < size; i += blockDim.x) r2c_cat[o + c2r_cat[o + i]] = i;
+    for (int i = threadIdx.x; i < size; i += blockDim.x) {
+        const int r = c2r_cat[o + i];
+        if (r < 0 || r >= size) {   // never expected: report instead of writing out of bounds
+            raise_error(err, kDevErrBadState);
+            continue;
+        }
+        r2c_cat[o + r] = i;
+    }
 }
 
 __global__ void identity_fill_kernel(int32_t *__restrict__ c2r_cat, const int64_t *__restrict__ out_off,
@@ -64,7 +71,9 @@ struct slcs_batch {
 
 namespace {
 
-int batch_step(slcs_batch *bt, cudaStream_t s) {
+int batch_step(slcs_batch *bt, cudaStream_t s, bool capturing) {
+    // inside a capture the timing events must become external event-record nodes of the graph
+    const unsigned evflags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     const int np = bt->npairs;
     SLCS_CUDA_TRY(cudaMemsetAsync(bt->dprog, 0, sizeof(int32_t) * std::max<int64_t>(bt->prog_total, 1), s));
     SLCS_CUDA_TRY(cudaMemsetAsync(bt->dsc, 0, sizeof(int32_t) * np, s));
@@ -75,7 +84,7 @@ int batch_step(slcs_batch *bt, cudaStream_t s) {
                                                                    (int) bt->empty.size());
         SLCS_CUDA_TRY(cudaGetLastError());
     }
-    SLCS_CUDA_TRY(cudaEventRecord(bt->ev0, s));
+    SLCS_CUDA_TRY(cudaEventRecordWithFlags(bt->ev0, s, evflags));
     const int nl = (int) bt->item_begin.size() - 1;
     for (int l = 0; l < nl; ++l) {
         const int cnt = bt->item_begin[l + 1] - bt->item_begin[l];
@@ -83,8 +92,8 @@ int batch_step(slcs_batch *bt, cudaStream_t s) {
         SLCS_TRY(launch_comb<uint8_t>(bt->dpairs, bt->ditems + bt->item_begin[l], cnt, bt->dnext + l, bt->derr,
                                       bt->resident, s));
     }
-    SLCS_CUDA_TRY(cudaEventRecord(bt->ev1, s));
-    invert_batch_kernel<<<np, 256, 0, s>>>(bt->dc2r, bt->doff, bt->dr2c);
+    SLCS_CUDA_TRY(cudaEventRecordWithFlags(bt->ev1, s, evflags));
+    invert_batch_kernel<<<np, 256, 0, s>>>(bt->dc2r, bt->doff, bt->dr2c, bt->derr);
     SLCS_CUDA_TRY(cudaGetLastError());
     return SLCS_OK;
 }
@@ -234,12 +243,12 @@ int slcs_batch_run(slcs_batch *bt, int use_graph, void *stream) {
     Engine *E;
     SLCS_TRY(engine(&E));
     cudaStream_t s = stream ? (cudaStream_t) stream : E->stream;
-    if (!use_graph) return batch_step(bt, s);
+    if (!use_graph) return batch_step(bt, s, false);
     if (!bt->gexec) {
         cudaStream_t cap;
         SLCS_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
         SLCS_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-        int rc = batch_step(bt, cap);
+        int rc = batch_step(bt, cap, true);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(cap, &g);
         cudaStreamDestroy(cap);

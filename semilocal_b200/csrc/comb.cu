@@ -137,9 +137,14 @@ __global__ void __launch_bounds__(128, 3) comb_kernel(const CombPair *__restrict
     }
 }
 
-__global__ void invert_kernel(const int32_t *__restrict__ c2r, int size, int32_t *__restrict__ r2c, int rot) {
+__global__ void invert_kernel(const int32_t *__restrict__ c2r, int size, int32_t *__restrict__ r2c, int rot,
+                              int *err) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < size; i += gridDim.x * blockDim.x) {
         const int r = c2r[i];
+        if (r < 0 || r >= size) {   // never expected: report instead of writing out of bounds
+            raise_error(err, kDevErrBadState);
+            continue;
+        }
         if (rot) r2c[size - 1 - r] = size - 1 - i;
         else r2c[r] = i;
     }
@@ -192,11 +197,11 @@ int comb_resident_warps(Engine *E) {
     return per_sm * 4 * E->num_sms;
 }
 
-int launch_invert(const int32_t *c2r, int size, int32_t *r2c, bool rot180, cudaStream_t s) {
+int launch_invert(const int32_t *c2r, int size, int32_t *r2c, bool rot180, int *d_err, cudaStream_t s) {
     if (size <= 0) return SLCS_OK;
     int blocks = (size + 255) / 256;
     if (blocks > 4096) blocks = 4096;
-    invert_kernel<<<blocks, 256, 0, s>>>(c2r, size, r2c, rot180 ? 1 : 0);
+    invert_kernel<<<blocks, 256, 0, s>>>(c2r, size, r2c, rot180 ? 1 : 0, d_err);
     SLCS_CUDA_TRY(cudaGetLastError());
     return SLCS_OK;
 }

@@ -140,6 +140,6 @@ int launch_comb(const CombPair *d_pairs, const CombItem *d_items, int nitems, in
 // Warps that fit on the device at once for the combing kernel.
 int comb_resident_warps(Engine *E);
 // c2r -> r2c for one pair (optionally rotated by 180 degrees), and the batched version.
-int launch_invert(const int32_t *c2r, int size, int32_t *r2c, bool rot180, cudaStream_t s);
+int launch_invert(const int32_t *c2r, int size, int32_t *r2c, bool rot180, int *d_err, cudaStream_t s);
 
 }  // namespace slcs
