@@ -53,6 +53,7 @@ SIGNATURES = {
     "slcs_comb_u8": [_u8p, _int, _u8p, _int, _i32p, _i32p, _i32p, _optp],
     "slcs_comb_i32": [_i32p, _int, _i32p, _int, _i32p, _i32p, _i32p, _optp],
     "slcs_comb_u8_dev": [_vp, _int, _vp, _int, _vp, _vp, _vp, _optp, _vp],
+    "slcs_comb_u8_dev_noalloc": [_vp, _int, _vp, _int, _vp, _vp, _vp, _vp],
     "slcs_lcs_u8": [_u8p, _int, _u8p, _int, _i32p],
     "slcs_bitcomb_llcs_u8": [_u8p, _int, _u8p, _int, _i32p],
     "slcs_bitcomb_llcs_u8_dev": [_vp, _int, _vp, _int, _vp, _vp],

@@ -189,13 +189,17 @@ int launch_comb(const CombPair *d_pairs, const CombItem *d_items, int nitems, in
 template int launch_comb<uint8_t>(const CombPair *, const CombItem *, int, int *, int *, int, cudaStream_t);
 template int launch_comb<int32_t>(const CombPair *, const CombItem *, int, int *, int *, int, cudaStream_t);
 
-int comb_resident_warps(Engine *E) {
+int comb_resident_warps_sm(int num_sms) {
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, comb_kernel<uint8_t>, 128, 0) != cudaSuccess ||
-        per_sm <= 0)
-        per_sm = 4;
-    return per_sm * 4 * E->num_sms;
+        per_sm <= 0) {
+        cudaGetLastError();
+        per_sm = 3;
+    }
+    return per_sm * 4 * num_sms;
 }
+
+int comb_resident_warps(Engine *E) { return comb_resident_warps_sm(E->num_sms); }
 
 int launch_invert(const int32_t *c2r, int size, int32_t *r2c, bool rot180, int *d_err, cudaStream_t s) {
     if (size <= 0) return SLCS_OK;

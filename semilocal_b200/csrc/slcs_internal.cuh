@@ -139,6 +139,7 @@ int launch_comb(const CombPair *d_pairs, const CombItem *d_items, int nitems, in
                 int grid_warps, cudaStream_t s);
 // Warps that fit on the device at once for the combing kernel.
 int comb_resident_warps(Engine *E);
+int comb_resident_warps_sm(int num_sms);
 // c2r -> r2c for one pair (optionally rotated by 180 degrees), and the batched version.
 int launch_invert(const int32_t *c2r, int size, int32_t *r2c, bool rot180, int *d_err, cudaStream_t s);
 
