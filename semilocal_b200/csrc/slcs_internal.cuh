@@ -143,4 +143,13 @@ int comb_resident_warps_sm(int num_sms);
 // c2r -> r2c for one pair (optionally rotated by 180 degrees), and the batched version.
 int launch_invert(const int32_t *c2r, int size, int32_t *r2c, bool rot180, int *d_err, cudaStream_t s);
 
+// ------------------------------------------------------------------------------------------------
+// steady ant (steady_ant.cu)
+// ------------------------------------------------------------------------------------------------
+// Batched unit-Monge products on device memory: problem i occupies [off[i], off[i] + n[i]) of the
+// concatenated row->col arrays d_P, d_Q and d_R (out).
+int steady_ant_batch_dev(const int32_t *d_P, const int32_t *d_Q, const std::vector<int64_t> &off,
+                         const std::vector<int> &n, int32_t *d_R, int *d_err, cudaStream_t s);
+int steady_ant_max_small();
+
 }  // namespace slcs

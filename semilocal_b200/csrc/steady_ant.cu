@@ -1,0 +1,780 @@
+// steady_ant.cu -- unit-Monge (sticky braid) multiplication R = P (.) Q on sm_100a.
+//
+// Same recursion as the reference's steady ant (R:common/include/Permutations/MongeMultuplicationStrategy.h:
+// 487-593): split the common index into two halves, multiply the halves, map them back (inverseMapping
+// :208-220) and combine them along the demarcation line (antPassage :244-301, restoreMatrixInRlo :304-323).
+// The product is unique, so the tree of splits is free to choose; here it is the bottom-up tree of aligned
+// power-of-two ranges of the common index, evaluated level by level:
+//   * node J = [lo, hi) of the common index keeps PL = rows of P whose column lies in J (sorted), QL = columns
+//     of Q whose row lies in J (sorted), and RES = the node's product in node-local coordinates;
+//   * a leaf j has PL = {P^-1(j)}, QL = {Q(j)}, RES = {(0, 0)};
+//   * merging the children is a merge of sorted lists (the positions are the reference's row/column mappers)
+//     followed by the ant passage.
+// The ant passage is restated data-parallel: for a node of size k with combined points (row r -> x_r, lo/hi)
+//   delta(r, c) = #{hi points: row < r, col < c} - #{lo points: row >= r, col >= c}
+// (the reference's rhi - rlo, BOTTOM_RIGHT / TOP_LEFT dominance sums, R:common/include/Permutations/
+// DominanceSum.h:210-294), c*(r) = min{c : delta(r, c) >= 0}, and the product keeps x_r in row r except where
+// 1 <= c*(r) <= k and the row's point lies on the wrong side of c*(r) (a hi point left of it or a lo point at
+// or right of it): there the point moves to column c*(r) - 1 (the reference's "good points").  Row by row,
+// c*(r) = c*(r+1) unless row r's point flips the sign, else one past the next column whose point raises
+// delta(r, .).  c* at every 32nd row is found by warp-wide ballot scans; the rows between are walked by one
+// thread each.
+#include <algorithm>
+#include <numeric>
+
+#include "slcs_internal.cuh"
+
+namespace slcs {
+namespace {
+
+constexpr int kSaSB = 4096;      // largest subtree a CTA finishes in shared memory
+constexpr int kSaThreads = 256;
+constexpr int kSaSF = 32;        // rows per walk (fine band)
+constexpr int kSaSC = 512;       // rows per coarse band (full-scan boundaries)
+constexpr int kSaPerThread = kSaSB / kSaThreads;
+
+struct SaBlockItem {
+    int64_t off;   // first common index of the block (concatenated problem layout)
+    int nb;        // block size (<= kSaSB)
+    int pad;
+};
+
+struct SaShared {
+    int32_t PL[kSaSB];
+    int32_t QL[kSaSB];
+    uint16_t RES[kSaSB];
+    uint16_t posP[kSaSB];
+    uint16_t posQ[kSaSB];
+    uint16_t xs[kSaSB];   // node-local row -> col | hi << 15
+    uint16_t ys[kSaSB];   // node-local col -> row | hi << 15
+    int32_t cst[kSaSB / kSaSF + 8];
+};
+
+__device__ __forceinline__ int count_less(const int32_t *arr, int lo, int hi, int32_t v) {
+    // number of entries < v in the sorted range arr[lo, hi)
+    int l = lo, h = hi;
+    while (l < h) {
+        const int mid = (l + h) >> 1;
+        if (arr[mid] < v) l = mid + 1;
+        else h = mid;
+    }
+    return l - lo;
+}
+
+// warp-wide: number of rows r in [r0, r1) of the node at base a whose point raises delta when moving up
+// past it at column c (rowind(r, c) = hi ? x < c : x >= c)
+__device__ __forceinline__ int warp_row_count(const SaShared &S, int a, int r0, int r1, int c, int lane) {
+    int total = 0;
+    for (int r = r0; r < r1; r += 32) {
+        const int rr = r + lane;
+        bool q = false;
+        if (rr < r1) {
+            const int v = S.xs[a + rr];
+            const int x = v & 0x7fff;
+            q = (v >> 15) ? (x < c) : (x >= c);
+        }
+        total += __popc(__ballot_sync(kFull, q));
+    }
+    return total;
+}
+
+// warp-wide: one past the need-th column g >= from whose point raises delta in row R
+// (colind(g, R) = hi ? y < R : y >= R); k + 1 when there is none
+__device__ __forceinline__ int warp_col_search(const SaShared &S, int a, int k, int from, int need, int R, int lane) {
+    if (need <= 0) return from;
+    for (int g0 = from; g0 < k; g0 += 32) {
+        const int g = g0 + lane;
+        bool q = false;
+        if (g < k) {
+            const int w = S.ys[a + g];
+            const int y = w & 0x7fff;
+            q = (w >> 15) ? (y < R) : (y >= R);
+        }
+        const unsigned mask = __ballot_sync(kFull, q);
+        const int cnt = __popc(mask);
+        if (need <= cnt) return g0 + (int) __fns(mask, 0, need) + 1;
+        need -= cnt;
+    }
+    return k + 1;
+}
+
+// flat task index -> (node, task within node); full nodes have per_full tasks, the trailing node the rest
+__device__ __forceinline__ void task_node(int t, int per_full, int nfull, int &nd, int &jj) {
+    if (t < nfull * per_full) {
+        nd = t / per_full;
+        jj = t - nd * per_full;
+    } else {
+        nd = nfull;
+        jj = t - nfull * per_full;
+    }
+}
+
+// one thread: rows [top, bot) of the node at base a, walking up from c = c*(bot)
+__device__ __forceinline__ void thread_walk(SaShared &S, int a, int k, int top, int bot, int c) {
+    for (int r = bot - 1; r >= top; --r) {
+        const int v = S.xs[a + r];
+        const int xr = v & 0x7fff;
+        const bool hi = v >> 15;
+        const bool ind = hi ? (xr < c) : (xr >= c);
+        if (ind) {
+            int g = c;
+            for (; g < k; ++g) {
+                const int w = S.ys[a + g];
+                const int yr = w & 0x7fff;
+                if ((w >> 15) ? (yr < r) : (yr >= r)) break;
+            }
+            c = g < k ? g + 1 : k + 1;
+        }
+        const bool good = c >= 1 && c <= k && (hi ? (xr < c) : (xr >= c));
+        S.RES[a + r] = (uint16_t) (good ? c - 1 : xr);
+    }
+}
+
+__global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *__restrict__ Pinv,
+                                                             const int32_t *__restrict__ Q,
+                                                             const SaBlockItem *__restrict__ items,
+                                                             int32_t *__restrict__ PLout, int32_t *__restrict__ QLout,
+                                                             int32_t *__restrict__ RESout, int *err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SaShared &S = *reinterpret_cast<SaShared *>(smem_raw);
+    const SaBlockItem it = items[blockIdx.x];
+    const int nb = it.nb;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = kSaThreads / 32;
+    for (int e = tid; e < nb; e += kSaThreads) {
+        S.PL[e] = Pinv[it.off + e];
+        S.QL[e] = Q[it.off + e];
+        S.RES[e] = 0;
+    }
+    __syncthreads();
+    for (int size = 1; size < nb; size <<= 1) {
+        const int span = size << 1;
+        // ---- merge the children's lists: positions in the parent lists ----
+        for (int e = tid; e < nb; e += kSaThreads) {
+            const int a = e & ~(span - 1);
+            const int m = min(a + size, nb), b = min(a + span, nb);
+            int pp, pq;
+            if (m >= b) {
+                pp = pq = e - a;
+            } else if (e < m) {
+                pp = (e - a) + count_less(S.PL, m, b, S.PL[e]);
+                pq = (e - a) + count_less(S.QL, m, b, S.QL[e]);
+            } else {
+                pp = (e - m) + count_less(S.PL, a, m, S.PL[e]);
+                pq = (e - m) + count_less(S.QL, a, m, S.QL[e]);
+            }
+            S.posP[e] = (uint16_t) pp;
+            S.posQ[e] = (uint16_t) pq;
+        }
+        __syncthreads();
+        // ---- children's products in the parent's coordinates (inverse mapping) ----
+        for (int e = tid; e < nb; e += kSaThreads) {
+            const int a = e & ~(span - 1);
+            const int m = min(a + size, nb), b = min(a + span, nb);
+            if (m >= b) continue;
+            const bool hi = e >= m;
+            const int cs = hi ? m : a;
+            const int rc = S.RES[e];
+            if (rc >= (hi ? b - m : m - a)) {   // never expected: report, keep shared accesses in bounds
+                raise_error(err, kDevErrBadState);
+                continue;
+            }
+            const int row = S.posP[e];
+            const int col = S.posQ[cs + rc];
+            S.xs[a + row] = (uint16_t) (col | (hi ? 0x8000 : 0));
+            S.ys[a + col] = (uint16_t) (row | (hi ? 0x8000 : 0));
+        }
+        // ---- reorder the lists in place (values staged in registers, one list at a time) ----
+        int32_t v[kSaPerThread];
+#pragma unroll
+        for (int i = 0; i < kSaPerThread; ++i) {
+            const int e = tid + i * kSaThreads;
+            if (e < nb) v[i] = S.PL[e];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kSaPerThread; ++i) {
+            const int e = tid + i * kSaThreads;
+            if (e < nb) S.PL[(e & ~(span - 1)) + S.posP[e]] = v[i];
+        }
+#pragma unroll
+        for (int i = 0; i < kSaPerThread; ++i) {
+            const int e = tid + i * kSaThreads;
+            if (e < nb) v[i] = S.QL[e];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kSaPerThread; ++i) {
+            const int e = tid + i * kSaThreads;
+            if (e < nb) S.QL[(e & ~(span - 1)) + S.posQ[e]] = v[i];
+        }
+        __syncthreads();
+        // ---- ant passage for every node of this level that has two children ----
+        const int nfull = nb / span;                  // nodes of size span
+        const int rem = nb - nfull * span;            // size of the trailing node
+        const int nnodes = nfull + (rem > size ? 1 : 0);
+        if (span > kSaSF) {
+            // phase A: coarse boundaries (multiples of kSaSC inside each node), full scans
+            const int ca_full = (span - 1) / kSaSC;
+            const int ca_last = rem > size ? (rem - 1) / kSaSC : 0;
+            for (int t = warp; t < nfull * ca_full + ca_last; t += nwarps) {
+                int nd, jj;
+                task_node(t, ca_full, nfull, nd, jj);
+                const int a = nd * span, k = nd < nfull ? span : rem;
+                const int R = (jj + 1) * kSaSC;
+                const int need = warp_row_count(S, a, R, k, 0, lane);   // lo rows at or below R
+                const int cst = warp_col_search(S, a, k, 0, need, R, lane);
+                if (lane == 0) S.cst[(a + R) / kSaSF] = cst;
+            }
+            __syncthreads();
+            // phase B: fine boundaries (multiples of kSaSF, not of kSaSC), band-restricted scans
+            const int fb_full = (span - 1) / kSaSF;
+            const int fb_last = rem > size ? (rem - 1) / kSaSF : 0;
+            for (int t = warp; t < nfull * fb_full + fb_last; t += nwarps) {
+                int nd, jj;
+                task_node(t, fb_full, nfull, nd, jj);
+                const int a = nd * span, k = nd < nfull ? span : rem;
+                const int R = (jj + 1) * kSaSF;
+                if (R % kSaSC == 0) continue;
+                const int Rb = min((R / kSaSC + 1) * kSaSC, k);
+                const int cb = Rb >= k ? 0 : S.cst[(a + Rb) / kSaSF];
+                int cst = k + 1;
+                if (cb <= k) {
+                    const int need = warp_row_count(S, a, R, Rb, cb, lane);
+                    cst = warp_col_search(S, a, k, cb, need, R, lane);
+                }
+                if (lane == 0) S.cst[(a + R) / kSaSF] = cst;
+            }
+            __syncthreads();
+            // phase C: walks of kSaSF rows, each from the c* of its bottom boundary
+            const int wb_full = (span + kSaSF - 1) / kSaSF;
+            const int wb_last = rem > size ? (rem + kSaSF - 1) / kSaSF : 0;
+            for (int t = tid; t < nfull * wb_full + wb_last; t += kSaThreads) {
+                int nd, jj;
+                task_node(t, wb_full, nfull, nd, jj);
+                const int a = nd * span, k = nd < nfull ? span : rem;
+                const int top = jj * kSaSF, bot = min(top + kSaSF, k);
+                const int c = bot >= k ? 0 : S.cst[(a + bot) / kSaSF];
+                thread_walk(S, a, k, top, bot, c);
+            }
+        } else {
+            for (int node = tid; node < nnodes; node += kSaThreads) {
+                const int a = node * span;
+                const int k = node < nfull ? span : rem;
+                thread_walk(S, a, k, 0, k, 0);
+            }
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < nb; e += kSaThreads) {
+        PLout[it.off + e] = S.PL[e];
+        QLout[it.off + e] = S.QL[e];
+        RESout[it.off + e] = S.RES[e];
+    }
+}
+
+// ------------------------------------------------------------------------------------------------------
+// Levels above the shared-memory block: nodes of k > kSaSB common indices, held in global memory.
+// ------------------------------------------------------------------------------------------------------
+constexpr int kMT = 2048;        // merge tile (output elements per CTA)
+constexpr int kHSF = 64;         // rows per walk at HBM levels
+constexpr unsigned kHiBit = 1u << 30;
+constexpr int kValMask = (1 << 30) - 1;
+
+struct SaNode {
+    int64_t off;       // first common index of the node
+    int k;             // node size
+    int h;             // size of the lo child (k - h = hi child)
+    int Sc;            // coarse band (rows/cols per table block), multiple of kHSF
+    int G;             // table blocks per dimension: ceil(k / Sc)
+    int64_t tab_off;   // offset of the node's (G+1) x (G+1) prefix table
+    int64_t vec_off;   // offset of the node's lo-row / lo-col counts (G+1 each)
+    int64_t cst_off;   // offset of the node's c* slots (k / kHSF + 1)
+};
+
+struct SaTile {
+    int node;
+    int t;      // tile index inside the node
+};
+
+__device__ __forceinline__ int merge_path(const int32_t *lo, int nlo, const int32_t *hi, int nhi, int diag) {
+    int l = max(0, diag - nhi), h = min(diag, nlo);
+    while (l < h) {
+        const int mid = (l + h) >> 1;
+        if (lo[mid] < hi[diag - 1 - mid]) l = mid + 1;
+        else h = mid;
+    }
+    return l;
+}
+
+// Merge the children's sorted lists of every node; pos receives the node-local parent position of every
+// child element (the reference's row / column mappers).
+__global__ void __launch_bounds__(256) sa_merge_kernel(const SaNode *__restrict__ nodes, const SaTile *__restrict__ tiles,
+                                                       const int32_t *__restrict__ Lin, int32_t *__restrict__ Lout,
+                                                       int32_t *__restrict__ pos) {
+    __shared__ int32_t sm_lo[kMT], sm_hi[kMT];
+    __shared__ int split[2];
+    const SaTile tl = tiles[blockIdx.x];
+    const SaNode nd = nodes[tl.node];
+    const int32_t *lo = Lin + nd.off, *hi = Lin + nd.off + nd.h;
+    const int nlo = nd.h, nhi = nd.k - nd.h;
+    const int o0 = tl.t * kMT, o1 = min(o0 + kMT, nd.k);
+    if (threadIdx.x == 0) {
+        split[0] = merge_path(lo, nlo, hi, nhi, o0);
+        split[1] = merge_path(lo, nlo, hi, nhi, o1);
+    }
+    __syncthreads();
+    const int i0 = split[0], i1 = split[1], j0 = o0 - i0, j1 = o1 - i1;
+    const int na = i1 - i0, nbb = j1 - j0;
+    for (int x = threadIdx.x; x < na; x += blockDim.x) sm_lo[x] = lo[i0 + x];
+    for (int x = threadIdx.x; x < nbb; x += blockDim.x) sm_hi[x] = hi[j0 + x];
+    __syncthreads();
+    for (int x = threadIdx.x; x < na; x += blockDim.x) {
+        const int v = sm_lo[x];
+        const int p = o0 + x + count_less(sm_hi, 0, nbb, v);
+        Lout[nd.off + p] = v;
+        pos[nd.off + i0 + x] = p;
+    }
+    for (int x = threadIdx.x; x < nbb; x += blockDim.x) {
+        const int v = sm_hi[x];
+        const int p = o0 + x + count_less(sm_lo, 0, na, v);
+        Lout[nd.off + p] = v;
+        pos[nd.off + nd.h + j0 + x] = p;
+    }
+}
+
+// Children's products in the parent's coordinates, signed block counts (hi +1, lo -1), lo-row / lo-col counts.
+__global__ void __launch_bounds__(256) sa_map_kernel(const SaNode *__restrict__ nodes, const SaTile *__restrict__ tiles,
+                                                     const int32_t *__restrict__ posP, const int32_t *__restrict__ posQ,
+                                                     const int32_t *__restrict__ RES, int32_t *__restrict__ xs,
+                                                     int32_t *__restrict__ ys, int32_t *__restrict__ tab,
+                                                     int32_t *__restrict__ vec, int *err) {
+    const SaTile tl = tiles[blockIdx.x];
+    const SaNode nd = nodes[tl.node];
+    const int e0 = tl.t * kMT, e1 = min(e0 + kMT, nd.k);
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const bool hi = e >= nd.h;
+        const int cs = hi ? nd.h : 0;
+        const int rc = RES[nd.off + e];
+        if (rc < 0 || rc >= (hi ? nd.k - nd.h : nd.h)) {
+            raise_error(err, kDevErrBadState);
+            continue;
+        }
+        const int row = posP[nd.off + e];
+        const int col = posQ[nd.off + cs + rc];
+        xs[nd.off + row] = col | (hi ? kHiBit : 0);
+        ys[nd.off + col] = row | (hi ? kHiBit : 0);
+        const int g = row / nd.Sc, hh = col / nd.Sc;
+        atomicAdd(&tab[nd.tab_off + (int64_t) g * (nd.G + 1) + hh], hi ? 1 : -1);
+        if (!hi) {
+            atomicAdd(&vec[nd.vec_off + g], 1);                  // lo rows per row block
+            atomicAdd(&vec[nd.vec_off + (nd.G + 1) + hh], 1);    // lo cols per col block
+        }
+    }
+}
+
+// Exclusive prefix sums of the block counts: along h for every row g (dir 0), then along g for every
+// column h (dir 1); the two lo-count vectors are scanned by the dir-0 lines G+1 and G+2.
+__global__ void __launch_bounds__(256) sa_scan_kernel(const SaNode *__restrict__ nodes, const int2 *__restrict__ lines,
+                                                      int32_t *__restrict__ tab, int32_t *__restrict__ vec, int dir) {
+    const int2 ln = lines[blockIdx.x];   // (node, line index)
+    const SaNode nd = nodes[ln.x];
+    const int W = nd.G + 1;
+    int32_t *base;
+    int64_t stride;
+    if (ln.y < W) {
+        base = tab + nd.tab_off + (dir == 0 ? (int64_t) ln.y * W : ln.y);
+        stride = dir == 0 ? 1 : W;
+    } else {
+        base = vec + nd.vec_off + (int64_t) (ln.y - W) * W;
+        stride = 1;
+    }
+    __shared__ int32_t warp_sums[8];
+    __shared__ int32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int c0 = 0; c0 < W; c0 += blockDim.x) {
+        const int c = c0 + threadIdx.x;
+        const int v = c < W ? base[c * stride] : 0;
+        int incl = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int o = __shfl_up_sync(kFull, incl, d);
+            if (lane >= d) incl += o;
+        }
+        if (lane == 31) warp_sums[warp] = incl;
+        __syncthreads();
+        int woff = 0;
+        for (int w = 0; w < warp; ++w) woff += warp_sums[w];
+        const int excl = carry + woff + incl - v;
+        __syncthreads();
+        if (c < W) base[c * stride] = excl;
+        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ int hbm_delta_corner(const SaNode &nd, const int32_t *tab, const int32_t *vec, int g, int h) {
+    // delta(g Sc, h Sc) = #{hi: row < g Sc, col < h Sc} - #{lo: row < g Sc, col < h Sc}
+    //                    + #{lo: row < g Sc} + #{lo: col < h Sc} - #lo       (tab holds the signed prefix)
+    const int W = nd.G + 1;
+    return tab[nd.tab_off + (int64_t) g * W + h] + vec[nd.vec_off + g] + vec[nd.vec_off + W + h] - nd.h;
+}
+
+__device__ __forceinline__ int hbm_row_count(const int32_t *xs, int64_t off, int r0, int r1, int c, int lane) {
+    int total = 0;
+    for (int r = r0; r < r1; r += 32) {
+        const int rr = r + lane;
+        bool q = false;
+        if (rr < r1) {
+            const int v = xs[off + rr];
+            const int x = v & kValMask;
+            q = (v & kHiBit) ? (x < c) : (x >= c);
+        }
+        total += __popc(__ballot_sync(kFull, q));
+    }
+    return total;
+}
+
+__device__ __forceinline__ int hbm_col_search(const int32_t *ys, int64_t off, int k, int from, int need, int R, int lane) {
+    if (need <= 0) return from;
+    for (int g0 = from; g0 < k; g0 += 32) {
+        const int g = g0 + lane;
+        bool q = false;
+        if (g < k) {
+            const int w = ys[off + g];
+            const int y = w & kValMask;
+            q = (w & kHiBit) ? (y < R) : (y >= R);
+        }
+        const unsigned mask = __ballot_sync(kFull, q);
+        const int cnt = __popc(mask);
+        if (need <= cnt) return g0 + (int) __fns(mask, 0, need) + 1;
+        need -= cnt;
+    }
+    return k + 1;
+}
+
+// c* at the coarse boundaries R = g Sc (one warp each): the table locates the column block, a ballot scan
+// of at most Sc columns finds the column.
+__global__ void __launch_bounds__(256) sa_coarse_kernel(const SaNode *__restrict__ nodes, const int2 *__restrict__ tasks,
+                                                        int ntasks, const int32_t *__restrict__ tab,
+                                                        const int32_t *__restrict__ vec, const int32_t *__restrict__ ys,
+                                                        int32_t *__restrict__ cst) {
+    const int lane = threadIdx.x & 31;
+    const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (t >= ntasks) return;
+    const int2 tk = tasks[t];   // (node, g)
+    const SaNode nd = nodes[tk.x];
+    const int g = tk.y, R = g * nd.Sc;
+    int l = 0, hgh = nd.G + 1;   // first h with delta(R, min(h Sc, k)) >= 0
+    while (l < hgh) {
+        const int mid = (l + hgh) >> 1;
+        if (hbm_delta_corner(nd, tab, vec, g, mid) >= 0) hgh = mid;
+        else l = mid + 1;
+    }
+    int c;
+    if (l == 0) c = 0;
+    else if (l > nd.G) c = nd.k + 1;
+    else {
+        const int need = -hbm_delta_corner(nd, tab, vec, g, l - 1);
+        c = hbm_col_search(ys, nd.off, nd.k, (l - 1) * nd.Sc, need, R, lane);
+    }
+    if (lane == 0) cst[nd.cst_off + R / kHSF] = c;
+}
+
+// c* at the other multiples of kHSF (one warp each), from the coarse boundary below.
+__global__ void __launch_bounds__(256) sa_fine_kernel(const SaNode *__restrict__ nodes, const int2 *__restrict__ tasks,
+                                                      int ntasks, const int32_t *__restrict__ xs,
+                                                      const int32_t *__restrict__ ys, int32_t *__restrict__ cst) {
+    const int lane = threadIdx.x & 31;
+    const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (t >= ntasks) return;
+    const int2 tk = tasks[t];   // (node, R)
+    const SaNode nd = nodes[tk.x];
+    const int R = tk.y;
+    const int Rb = min((R / nd.Sc + 1) * nd.Sc, nd.k);
+    const int cb = Rb >= nd.k ? 0 : cst[nd.cst_off + Rb / kHSF];
+    int c = nd.k + 1;
+    if (cb <= nd.k) {
+        const int need = hbm_row_count(xs, nd.off, R, Rb, cb, lane);
+        c = hbm_col_search(ys, nd.off, nd.k, cb, need, R, lane);
+    }
+    if (lane == 0) cst[nd.cst_off + R / kHSF] = c;
+}
+
+// Walks of kHSF rows (one thread each) writing the node's product.
+__global__ void __launch_bounds__(256) sa_walk_kernel(const SaNode *__restrict__ nodes, const int2 *__restrict__ tasks,
+                                                      int ntasks, const int32_t *__restrict__ xs,
+                                                      const int32_t *__restrict__ ys, const int32_t *__restrict__ cst,
+                                                      int32_t *__restrict__ RESout) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntasks) return;
+    const int2 tk = tasks[t];   // (node, top row)
+    const SaNode nd = nodes[tk.x];
+    const int k = nd.k, top = tk.y, bot = min(top + kHSF, k);
+    int c = bot >= k ? 0 : cst[nd.cst_off + bot / kHSF];
+    for (int r = bot - 1; r >= top; --r) {
+        const int v = xs[nd.off + r];
+        const int xr = v & kValMask;
+        const bool hi = v & kHiBit;
+        if (hi ? (xr < c) : (xr >= c)) {
+            int g = c;
+            for (; g < k; ++g) {
+                const int w = ys[nd.off + g];
+                const int yr = w & kValMask;
+                if ((w & kHiBit) ? (yr < r) : (yr >= r)) break;
+            }
+            c = g < k ? g + 1 : k + 1;
+        }
+        const bool good = c >= 1 && c <= k && (hi ? (xr < c) : (xr >= c));
+        RESout[nd.off + r] = good ? c - 1 : xr;
+    }
+}
+
+// Nodes without a sibling at this level carry their lists and product over unchanged.
+__global__ void sa_copy_kernel(const int64_t *__restrict__ ranges, int nranges, const int32_t *__restrict__ a0,
+                               const int32_t *__restrict__ b0, const int32_t *__restrict__ c0, int32_t *__restrict__ a1,
+                               int32_t *__restrict__ b1, int32_t *__restrict__ c1) {
+    for (int r = blockIdx.y; r < nranges; r += gridDim.y) {
+        const int64_t off = ranges[2 * r], len = ranges[2 * r + 1];
+        for (int64_t i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (int64_t) gridDim.x * blockDim.x) {
+            a1[off + i] = a0[off + i];
+            b1[off + i] = b0[off + i];
+            c1[off + i] = c0[off + i];
+        }
+    }
+}
+
+// P^-1 of every problem: Pinv[off + P(r)] = r.
+__global__ void sa_pinv_kernel(const SaNode *__restrict__ probs, const SaTile *__restrict__ tiles,
+                               const int32_t *__restrict__ P, int32_t *__restrict__ Pinv, int *err) {
+    const SaTile tl = tiles[blockIdx.x];
+    const SaNode pr = probs[tl.node];
+    const int e0 = tl.t * kMT, e1 = min(e0 + kMT, pr.k);
+    for (int r = e0 + threadIdx.x; r < e1; r += blockDim.x) {
+        const int c = P[pr.off + r];
+        if (c < 0 || c >= pr.k) {
+            raise_error(err, kDevErrBadState);
+            continue;
+        }
+        Pinv[pr.off + c] = r;
+    }
+}
+
+}  // namespace
+
+// Batched steady ant on device memory: problems i = 0..np-1 occupy [off[i], off[i] + n[i]) of the
+// concatenated arrays d_P, d_Q (row -> col) and d_R (out).  off / n are host arrays.
+int steady_ant_batch_dev(const int32_t *d_P, const int32_t *d_Q, const std::vector<int64_t> &off,
+                         const std::vector<int> &n, int32_t *d_R, int *d_err, cudaStream_t s) {
+    const int np = (int) n.size();
+    int64_t total = 0;
+    int maxn = 0;
+    for (int i = 0; i < np; ++i) {
+        total = std::max<int64_t>(total, off[i] + n[i]);
+        maxn = std::max(maxn, n[i]);
+    }
+    if (total == 0) return SLCS_OK;
+    static bool attr_set = false;
+    if (!attr_set) {
+        SLCS_CUDA_TRY(cudaFuncSetAttribute(sa_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int) sizeof(SaShared)));
+        attr_set = true;
+    }
+    DevBuf<int32_t> pinv, plA, plB, qlA, qlB, resA, resB;
+    SLCS_TRY(pinv.alloc(total, s));
+    SLCS_TRY(plA.alloc(total, s));
+    SLCS_TRY(qlA.alloc(total, s));
+    SLCS_TRY(resA.alloc(total, s));
+    // P^-1 per problem, then the shared-memory subtrees
+    {
+        std::vector<SaTile> tiles;
+        std::vector<SaNode> probs(np);
+        std::vector<SaBlockItem> items;
+        for (int i = 0; i < np; ++i) {
+            probs[i] = SaNode{off[i], n[i], n[i], 0, 0, 0, 0, 0};
+            for (int t = 0; t * kMT < n[i]; ++t) tiles.push_back(SaTile{i, t});
+            for (int b0 = 0; b0 < n[i]; b0 += kSaSB) items.push_back(SaBlockItem{off[i] + b0, std::min(kSaSB, n[i] - b0), 0});
+        }
+        DevBuf<SaNode> dprobs;
+        DevBuf<SaTile> dtiles;
+        DevBuf<SaBlockItem> ditems;
+        SLCS_TRY(dprobs.alloc(np, s));
+        SLCS_TRY(dtiles.alloc(tiles.size(), s));
+        SLCS_TRY(ditems.alloc(items.size(), s));
+        SLCS_CUDA_TRY(cudaMemcpyAsync(dprobs.p, probs.data(), sizeof(SaNode) * np, cudaMemcpyHostToDevice, s));
+        SLCS_CUDA_TRY(cudaMemcpyAsync(dtiles.p, tiles.data(), sizeof(SaTile) * tiles.size(), cudaMemcpyHostToDevice, s));
+        SLCS_CUDA_TRY(cudaMemcpyAsync(ditems.p, items.data(), sizeof(SaBlockItem) * items.size(), cudaMemcpyHostToDevice, s));
+        if (!tiles.empty()) {
+            sa_pinv_kernel<<<(int) tiles.size(), 256, 0, s>>>(dprobs.p, dtiles.p, d_P, pinv.p, d_err);
+            SLCS_CUDA_TRY(cudaGetLastError());
+        }
+        if (!items.empty()) {
+            sa_block_kernel<<<(int) items.size(), kSaThreads, sizeof(SaShared), s>>>(pinv.p, d_Q, ditems.p, plA.p,
+                                                                                     qlA.p, resA.p, d_err);
+            SLCS_CUDA_TRY(cudaGetLastError());
+        }
+        // problems that fit one block are done
+        for (int i = 0; i < np; ++i)
+            if (n[i] > 0 && n[i] <= kSaSB)
+                SLCS_CUDA_TRY(cudaMemcpyAsync(d_R + off[i], resA.p + off[i], sizeof(int32_t) * n[i],
+                                              cudaMemcpyDeviceToDevice, s));
+        SLCS_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    if (maxn <= kSaSB) return SLCS_OK;
+
+    SLCS_TRY(plB.alloc(total, s));
+    SLCS_TRY(qlB.alloc(total, s));
+    SLCS_TRY(resB.alloc(total, s));
+    DevBuf<int32_t> posP, posQ, xs, ys;
+    SLCS_TRY(posP.alloc(total, s));
+    SLCS_TRY(posQ.alloc(total, s));
+    SLCS_TRY(xs.alloc(total, s));
+    SLCS_TRY(ys.alloc(total, s));
+    int32_t *PLc = plA.p, *PLn = plB.p, *QLc = qlA.p, *QLn = qlB.p, *Rc = resA.p, *Rn = resB.p;
+    for (int64_t size = kSaSB; size < maxn; size <<= 1) {
+        const int64_t span = size << 1;
+        std::vector<SaNode> nodes;
+        std::vector<int64_t> copies;
+        std::vector<int> finished;
+        int64_t tab_tot = 0, vec_tot = 0, cst_tot = 0;
+        for (int i = 0; i < np; ++i) {
+            if (n[i] <= size) continue;   // finished at an earlier level (or in the block kernel)
+            if (n[i] <= span) finished.push_back(i);
+            for (int64_t a = 0; a < n[i]; a += span) {
+                const int k = (int) std::min<int64_t>(span, n[i] - a);
+                const int h = (int) std::min<int64_t>(size, k);
+                if (h == k) {
+                    copies.push_back(off[i] + a);
+                    copies.push_back(k);
+                    continue;
+                }
+                int Sc = 256;
+                while ((int64_t) Sc * Sc < k) Sc <<= 1;
+                const int G = (k + Sc - 1) / Sc;
+                SaNode nd{off[i] + a, k, h, Sc, G, tab_tot, vec_tot, cst_tot};
+                tab_tot += (int64_t) (G + 1) * (G + 1);
+                vec_tot += 2 * (int64_t) (G + 1);
+                cst_tot += k / kHSF + 1;
+                nodes.push_back(nd);
+            }
+        }
+        std::vector<SaTile> tiles;
+        std::vector<int2> lines0, lines1, ctasks, ftasks, wtasks;
+        for (int j = 0; j < (int) nodes.size(); ++j) {
+            const SaNode &nd = nodes[j];
+            for (int t = 0; (int64_t) t * kMT < nd.k; ++t) tiles.push_back(SaTile{j, t});
+            for (int y = 0; y < nd.G + 3; ++y) lines0.push_back(make_int2(j, y));
+            for (int y = 0; y < nd.G + 1; ++y) lines1.push_back(make_int2(j, y));
+            for (int g = 1; g < nd.G; ++g) ctasks.push_back(make_int2(j, g));
+            for (int R = kHSF; R < nd.k; R += kHSF)
+                if (R % nd.Sc) ftasks.push_back(make_int2(j, R));
+            for (int top = 0; top < nd.k; top += kHSF) wtasks.push_back(make_int2(j, top));
+        }
+        DevBuf<SaNode> dnodes;
+        DevBuf<SaTile> dtiles;
+        DevBuf<int2> dl0, dl1, dct, dft, dwt;
+        DevBuf<int32_t> tab, vec, cst;
+        DevBuf<int64_t> dcopies;
+        if (!nodes.empty()) {
+            SLCS_TRY(dnodes.alloc(nodes.size(), s));
+            SLCS_TRY(dtiles.alloc(tiles.size(), s));
+            SLCS_TRY(dl0.alloc(lines0.size(), s));
+            SLCS_TRY(dl1.alloc(lines1.size(), s));
+            SLCS_TRY(dct.alloc(std::max<size_t>(ctasks.size(), 1), s));
+            SLCS_TRY(dft.alloc(std::max<size_t>(ftasks.size(), 1), s));
+            SLCS_TRY(dwt.alloc(wtasks.size(), s));
+            SLCS_TRY(tab.alloc(tab_tot, s));
+            SLCS_TRY(vec.alloc(vec_tot, s));
+            SLCS_TRY(cst.alloc(cst_tot, s));
+            SLCS_CUDA_TRY(cudaMemcpyAsync(dnodes.p, nodes.data(), sizeof(SaNode) * nodes.size(), cudaMemcpyHostToDevice, s));
+            SLCS_CUDA_TRY(cudaMemcpyAsync(dtiles.p, tiles.data(), sizeof(SaTile) * tiles.size(), cudaMemcpyHostToDevice, s));
+            SLCS_CUDA_TRY(cudaMemcpyAsync(dl0.p, lines0.data(), sizeof(int2) * lines0.size(), cudaMemcpyHostToDevice, s));
+            SLCS_CUDA_TRY(cudaMemcpyAsync(dl1.p, lines1.data(), sizeof(int2) * lines1.size(), cudaMemcpyHostToDevice, s));
+            if (!ctasks.empty())
+                SLCS_CUDA_TRY(cudaMemcpyAsync(dct.p, ctasks.data(), sizeof(int2) * ctasks.size(), cudaMemcpyHostToDevice, s));
+            if (!ftasks.empty())
+                SLCS_CUDA_TRY(cudaMemcpyAsync(dft.p, ftasks.data(), sizeof(int2) * ftasks.size(), cudaMemcpyHostToDevice, s));
+            SLCS_CUDA_TRY(cudaMemcpyAsync(dwt.p, wtasks.data(), sizeof(int2) * wtasks.size(), cudaMemcpyHostToDevice, s));
+            SLCS_CUDA_TRY(cudaMemsetAsync(tab.p, 0, sizeof(int32_t) * tab_tot, s));
+            SLCS_CUDA_TRY(cudaMemsetAsync(vec.p, 0, sizeof(int32_t) * vec_tot, s));
+            const int nt = (int) tiles.size();
+            sa_merge_kernel<<<nt, 256, 0, s>>>(dnodes.p, dtiles.p, PLc, PLn, posP.p);
+            sa_merge_kernel<<<nt, 256, 0, s>>>(dnodes.p, dtiles.p, QLc, QLn, posQ.p);
+            sa_map_kernel<<<nt, 256, 0, s>>>(dnodes.p, dtiles.p, posP.p, posQ.p, Rc, xs.p, ys.p, tab.p, vec.p, d_err);
+            sa_scan_kernel<<<(int) lines0.size(), 256, 0, s>>>(dnodes.p, dl0.p, tab.p, vec.p, 0);
+            sa_scan_kernel<<<(int) lines1.size(), 256, 0, s>>>(dnodes.p, dl1.p, tab.p, vec.p, 1);
+            if (!ctasks.empty())
+                sa_coarse_kernel<<<(int) ((ctasks.size() + 7) / 8), 256, 0, s>>>(dnodes.p, dct.p, (int) ctasks.size(),
+                                                                                  tab.p, vec.p, ys.p, cst.p);
+            if (!ftasks.empty())
+                sa_fine_kernel<<<(int) ((ftasks.size() + 7) / 8), 256, 0, s>>>(dnodes.p, dft.p, (int) ftasks.size(), xs.p,
+                                                                                ys.p, cst.p);
+            sa_walk_kernel<<<(int) ((wtasks.size() + 255) / 256), 256, 0, s>>>(dnodes.p, dwt.p, (int) wtasks.size(),
+                                                                               xs.p, ys.p, cst.p, Rn);
+            SLCS_CUDA_TRY(cudaGetLastError());
+        }
+        if (!copies.empty()) {
+            SLCS_TRY(dcopies.alloc(copies.size(), s));
+            SLCS_CUDA_TRY(cudaMemcpyAsync(dcopies.p, copies.data(), sizeof(int64_t) * copies.size(), cudaMemcpyHostToDevice, s));
+            dim3 grid(64, (unsigned) std::min<size_t>(copies.size() / 2, 65535));
+            sa_copy_kernel<<<grid, 256, 0, s>>>(dcopies.p, (int) (copies.size() / 2), PLc, QLc, Rc, PLn, QLn, Rn);
+            SLCS_CUDA_TRY(cudaGetLastError());
+        }
+        for (int i : finished)
+            SLCS_CUDA_TRY(cudaMemcpyAsync(d_R + off[i], Rn + off[i], sizeof(int32_t) * n[i], cudaMemcpyDeviceToDevice, s));
+        // the per-level task arrays are freed (stream-ordered) at the end of this scope
+        std::swap(PLc, PLn);
+        std::swap(QLc, QLn);
+        std::swap(Rc, Rn);
+        SLCS_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    return SLCS_OK;
+}
+
+int steady_ant_max_small() { return kSaSB; }
+
+}  // namespace slcs
+
+using namespace slcs;
+
+extern "C" {
+
+int slcs_steady_ant_dev(const int32_t *d_p, const int32_t *d_q, int n, int32_t *d_r, const slcs_opts *opts,
+                        void *stream) {
+    (void) opts;
+    if (n < 0) return fail(SLCS_ERR_ARG, "negative size");
+    if (n > 0 && (!d_p || !d_q || !d_r)) return fail(SLCS_ERR_ARG, "NULL buffer");
+    if (n >= (1 << 30)) return fail(SLCS_ERR_TOO_LARGE, "n must be below 2^30");
+    Engine *E;
+    SLCS_TRY(engine(&E));
+    if (n == 0) return SLCS_OK;
+    cudaStream_t s = stream ? (cudaStream_t) stream : E->stream;
+    DevBuf<int> err;
+    SLCS_TRY(err.alloc(1, s));
+    SLCS_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+    SLCS_TRY(steady_ant_batch_dev(d_p, d_q, std::vector<int64_t>{0}, std::vector<int>{n}, d_r, err.p, s));
+    return check_dev_err(err.p, s);
+}
+
+int slcs_steady_ant(const int32_t *p, const int32_t *q, int n, int32_t *r, const slcs_opts *opts) {
+    if (n < 0) return fail(SLCS_ERR_ARG, "negative size");
+    if (n > 0 && (!p || !q || !r)) return fail(SLCS_ERR_ARG, "NULL buffer");
+    if (n >= (1 << 30)) return fail(SLCS_ERR_TOO_LARGE, "n must be below 2^30");
+    Engine *E;
+    SLCS_TRY(engine(&E));
+    if (n == 0) return SLCS_OK;
+    cudaStream_t s = E->stream;
+    DevBuf<int32_t> dp, dq, dr;
+    SLCS_TRY(dp.alloc(n, s));
+    SLCS_TRY(dq.alloc(n, s));
+    SLCS_TRY(dr.alloc(n, s));
+    SLCS_CUDA_TRY(cudaMemcpyAsync(dp.p, p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    SLCS_CUDA_TRY(cudaMemcpyAsync(dq.p, q, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    SLCS_TRY(slcs_steady_ant_dev(dp.p, dq.p, n, dr.p, opts, s));
+    SLCS_CUDA_TRY(cudaMemcpyAsync(r, dr.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+    SLCS_CUDA_TRY(cudaStreamSynchronize(s));
+    return SLCS_OK;
+}
+
+}  // extern "C"
