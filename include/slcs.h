@@ -109,6 +109,17 @@ int slcs_steady_ant(const int32_t *p, const int32_t *q, int n, int32_t *r, const
 int slcs_steady_ant_dev(const int32_t *d_p, const int32_t *d_q, int n, int32_t *d_r, const slcs_opts *opts,
                         void *stream);
 
+/* Reusable steady-ant plan for size n (device-resident, graph-capturable): create() plans and allocates
+ * all scratch, run() only launches kernels on `stream` (with use_graph != 0 the launch sequence is
+ * captured once per (p, q, r) pointer triple and replayed), check() waits and reports the device error word. */
+typedef struct slcs_sa_plan slcs_sa_plan;
+int slcs_sa_plan_create(int n, slcs_sa_plan **out);
+int slcs_sa_plan_run(slcs_sa_plan *pl, const int32_t *d_p, const int32_t *d_q, int32_t *d_r, int use_graph,
+                     void *stream);
+int slcs_sa_plan_check(slcs_sa_plan *pl, void *stream);
+int slcs_sa_plan_launches(slcs_sa_plan *pl, int32_t *launches);
+int slcs_sa_plan_destroy(slcs_sa_plan *pl);
+
 /* Glue braid p (pm rows of a, pn columns of b) with braid q sharing k strands.
  * row_glue != 0: p above q (k = pn = qn); row_glue == 0: p left of q (k = pm = qm).
  * Replaces common::StaggeredStickyBraidMultiplication::staggeredStickyMultiplication<RowGlue>

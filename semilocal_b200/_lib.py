@@ -59,6 +59,11 @@ SIGNATURES = {
     "slcs_bitcomb_llcs_u8_dev": [_vp, _int, _vp, _int, _vp, _vp],
     "slcs_steady_ant": [_i32p, _i32p, _int, _i32p, _optp],
     "slcs_steady_ant_dev": [_vp, _vp, _int, _vp, _optp, _vp],
+    "slcs_sa_plan_create": [_int, ctypes.POINTER(_vp)],
+    "slcs_sa_plan_run": [_vp, _vp, _vp, _vp, _int, _vp],
+    "slcs_sa_plan_check": [_vp, _vp],
+    "slcs_sa_plan_launches": [_vp, _i32p],
+    "slcs_sa_plan_destroy": [_vp],
     "slcs_staggered_glue": [_i32p, _int, _int, _i32p, _int, _int, _int, _i32p],
     "slcs_scores": [_i32p, _int, _int, _qp, _int, _i32p],
     "slcs_scores_dev": [_vp, _int, _int, _vp, _int, _vp, _vp],

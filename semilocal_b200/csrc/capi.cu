@@ -132,6 +132,44 @@ int comb_wavefront_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int3
     return check_dev_err(err.p, s);
 }
 
+template <typename T>
+int comb_hybrid_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int32_t *d_r2c, int32_t *d_c2r,
+                    int32_t *d_score, const slcs_opts *opts, cudaStream_t s) {
+    const int tr = (opts && opts->tile_rows > 0) ? opts->tile_rows : 4096;
+    const int tc = (opts && opts->tile_cols > 0) ? opts->tile_cols : 4096;
+    HybridPlan *H = nullptr;
+    SLCS_TRY(hybrid_plan_create(m, n, tr, tc, E, s, &H));
+    DevBuf<int> err;
+    int rc = err.alloc(1, s);
+    if (rc == SLCS_OK && cudaMemsetAsync(err.p, 0, sizeof(int), s) != cudaSuccess) rc = fail(SLCS_ERR_CUDA, "memset");
+    if (rc == SLCS_OK) rc = hybrid_plan_run<T>(H, d_a, d_b, err.p, s);
+    if (rc == SLCS_OK && cudaMemcpyAsync(d_r2c, hybrid_result_r2c(H), sizeof(int32_t) * (m + n),
+                                         cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        rc = fail(SLCS_ERR_CUDA, "result copy");
+    if (rc == SLCS_OK && d_c2r && cudaMemcpyAsync(d_c2r, hybrid_result_c2r(H), sizeof(int32_t) * (m + n),
+                                                  cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        rc = fail(SLCS_ERR_CUDA, "result copy");
+    if (rc == SLCS_OK && d_score) rc = hybrid_score(H, d_score, s);
+    if (rc == SLCS_OK) rc = check_dev_err(err.p, s);
+    hybrid_plan_destroy(H);
+    return rc;
+}
+
+// Algorithm choice: the hybrid when asked for, or (AUTO) for grids large in both dimensions.
+bool use_hybrid(const slcs_opts *opts, int m, int n) {
+    const int algo = opts ? opts->algo : SLCS_ALGO_AUTO;
+    if (algo == SLCS_ALGO_HYBRID) return true;
+    if (algo == SLCS_ALGO_WAVEFRONT) return false;
+    return false;   // AUTO: the wavefront saturates the device once the pair has ~1000 bands; see DESIGN
+}
+
+template <typename T>
+int comb_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int32_t *d_r2c, int32_t *d_c2r, int32_t *d_score,
+             const slcs_opts *opts, cudaStream_t s) {
+    if (use_hybrid(opts, m, n)) return comb_hybrid_dev<T>(E, d_a, m, d_b, n, d_r2c, d_c2r, d_score, opts, s);
+    return comb_wavefront_dev<T>(E, d_a, m, d_b, n, d_r2c, d_c2r, d_score, opts, s);
+}
+
 int identity_host(int size, int32_t *r2c, int32_t *c2r, int32_t *score) {
     for (int i = 0; i < size; ++i) {
         if (r2c) r2c[i] = i;
@@ -161,7 +199,7 @@ int comb_host(const T *a, int m, const T *b, int n, int32_t *row_to_col, int32_t
     SLCS_CUDA_TRY(cudaMemcpyAsync(da.p, a, sizeof(T) * m, cudaMemcpyHostToDevice, s));
     SLCS_CUDA_TRY(cudaMemcpyAsync(db.p, b, sizeof(T) * n, cudaMemcpyHostToDevice, s));
     SLCS_CUDA_TRY(cudaMemsetAsync(dsc.p, 0, sizeof(int32_t), s));
-    SLCS_TRY(comb_wavefront_dev<T>(E, da.p, m, db.p, n, dr.p, col_to_row ? dc.p : nullptr, dsc.p, opts, s));
+    SLCS_TRY(comb_dev<T>(E, da.p, m, db.p, n, dr.p, col_to_row ? dc.p : nullptr, dsc.p, opts, s));
     SLCS_CUDA_TRY(cudaMemcpyAsync(row_to_col, dr.p, sizeof(int32_t) * (m + n), cudaMemcpyDeviceToHost, s));
     if (col_to_row)
         SLCS_CUDA_TRY(cudaMemcpyAsync(col_to_row, dc.p, sizeof(int32_t) * (m + n), cudaMemcpyDeviceToHost, s));
@@ -253,7 +291,7 @@ int slcs_comb_u8_dev(const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32
         }
         return SLCS_OK;
     }
-    return comb_wavefront_dev<uint8_t>(E, d_a, m, d_b, n, d_row_to_col, d_col_to_row, d_score, opts, s);
+    return comb_dev<uint8_t>(E, d_a, m, d_b, n, d_row_to_col, d_col_to_row, d_score, opts, s);
 }
 
 int slcs_lcs_u8(const uint8_t *a, int m, const uint8_t *b, int n, int32_t *score) {

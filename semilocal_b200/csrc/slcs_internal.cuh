@@ -151,5 +151,38 @@ int launch_invert(const int32_t *c2r, int size, int32_t *r2c, bool rot180, int *
 int steady_ant_batch_dev(const int32_t *d_P, const int32_t *d_Q, const std::vector<int64_t> &off,
                          const std::vector<int> &n, int32_t *d_R, int *d_err, cudaStream_t s);
 int steady_ant_max_small();
+// Reusable plans: create() plans and allocates, run() only launches kernels on s (capturable).
+struct SaPlan;
+// Per-element scratch that several plans run one after another can share (owned by the caller).
+struct SaScratch {
+    int32_t *b[11] = {};   // 11 arrays of `elems` int32
+    int32_t *tabp = nullptr, *vecp = nullptr, *cstp = nullptr;
+    int64_t elems = 0, tab = 0, vec = 0, cst = 0;
+};
+int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, SaPlan **out, cudaStream_t s,
+                   const SaScratch *shared);
+// shared != nullptr: the plan uses the caller's scratch; shared->elems < 0 defers the binding to sa_plan_bind.
+int sa_plan_bind(SaPlan *P, const SaScratch *shared);
+// Scratch sizes a plan needs (for building a shared SaScratch).
+void sa_plan_needs(const SaPlan *P, int64_t *elems, int64_t *tab, int64_t *vec, int64_t *cst);
+int sa_plan_run(SaPlan *P, const int32_t *d_P, const int32_t *d_Q, int32_t *d_R, int *d_err, cudaStream_t s);
+int sa_plan_run_ex(SaPlan *P, const int32_t *d_P, const int32_t *d_leafP, const int32_t *d_Q, int32_t *d_R,
+                   int32_t *d_PLout, int32_t *d_QLout, int *d_err, cudaStream_t s);
+void sa_plan_destroy(SaPlan *P);
+int sa_plan_launches(const SaPlan *P);
+int64_t sa_plan_total(const SaPlan *P);
+
+// ------------------------------------------------------------------------------------------------
+// hybrid (hybrid.cu)
+// ------------------------------------------------------------------------------------------------
+struct HybridPlan;
+int hybrid_plan_create(int m, int n, int tile_rows, int tile_cols, Engine *E, cudaStream_t s, HybridPlan **out);
+template <typename T>
+int hybrid_plan_run(HybridPlan *H, const T *d_a, const T *d_b, int *d_err, cudaStream_t s);
+void hybrid_plan_destroy(HybridPlan *H);
+int32_t *hybrid_result_r2c(HybridPlan *H);
+int32_t *hybrid_result_c2r(HybridPlan *H);
+int hybrid_score(HybridPlan *H, int32_t *d_score, cudaStream_t s);
+int hybrid_launches(const HybridPlan *H);
 
 }  // namespace slcs

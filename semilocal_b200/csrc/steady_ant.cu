@@ -561,86 +561,129 @@ __global__ void sa_pinv_kernel(const SaNode *__restrict__ probs, const SaTile *_
     }
 }
 
+
+struct SaLevel {
+    int64_t size;                 // children size at this level (node span = 2 size)
+    int nnodes, ntiles, nl0, nl1, nct, nft, nwt, ncopies;
+    int64_t o_nodes, o_tiles, o_l0, o_l1, o_ct, o_ft, o_wt, o_copies;   // offsets into the plan arrays
+    int64_t tab_tot, vec_tot, cst_tot;
+    std::vector<int> finished;    // problems whose root is produced at this level
+};
+
+
 }  // namespace
 
-// Batched steady ant on device memory: problems i = 0..np-1 occupy [off[i], off[i] + n[i]) of the
-// concatenated arrays d_P, d_Q (row -> col) and d_R (out).  off / n are host arrays.
-int steady_ant_batch_dev(const int32_t *d_P, const int32_t *d_Q, const std::vector<int64_t> &off,
-                         const std::vector<int> &n, int32_t *d_R, int *d_err, cudaStream_t s) {
-    const int np = (int) n.size();
+struct SaPlan {
+    std::vector<int64_t> off;
+    std::vector<int> n;
+    int np = 0;
     int64_t total = 0;
     int maxn = 0;
-    for (int i = 0; i < np; ++i) {
-        total = std::max<int64_t>(total, off[i] + n[i]);
-        maxn = std::max(maxn, n[i]);
-    }
-    if (total == 0) return SLCS_OK;
-    static bool attr_set = false;
-    if (!attr_set) {
-        SLCS_CUDA_TRY(cudaFuncSetAttribute(sa_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int) sizeof(SaShared)));
-        attr_set = true;
-    }
-    DevBuf<int32_t> pinv, plA, plB, qlA, qlB, resA, resB;
-    SLCS_TRY(pinv.alloc(total, s));
-    SLCS_TRY(plA.alloc(total, s));
-    SLCS_TRY(qlA.alloc(total, s));
-    SLCS_TRY(resA.alloc(total, s));
-    // P^-1 per problem, then the shared-memory subtrees
-    {
-        std::vector<SaTile> tiles;
-        std::vector<SaNode> probs(np);
-        std::vector<SaBlockItem> items;
-        for (int i = 0; i < np; ++i) {
-            probs[i] = SaNode{off[i], n[i], n[i], 0, 0, 0, 0, 0};
-            for (int t = 0; t * kMT < n[i]; ++t) tiles.push_back(SaTile{i, t});
-            for (int b0 = 0; b0 < n[i]; b0 += kSaSB) items.push_back(SaBlockItem{off[i] + b0, std::min(kSaSB, n[i] - b0), 0});
-        }
-        DevBuf<SaNode> dprobs;
-        DevBuf<SaTile> dtiles;
-        DevBuf<SaBlockItem> ditems;
-        SLCS_TRY(dprobs.alloc(np, s));
-        SLCS_TRY(dtiles.alloc(tiles.size(), s));
-        SLCS_TRY(ditems.alloc(items.size(), s));
-        SLCS_CUDA_TRY(cudaMemcpyAsync(dprobs.p, probs.data(), sizeof(SaNode) * np, cudaMemcpyHostToDevice, s));
-        SLCS_CUDA_TRY(cudaMemcpyAsync(dtiles.p, tiles.data(), sizeof(SaTile) * tiles.size(), cudaMemcpyHostToDevice, s));
-        SLCS_CUDA_TRY(cudaMemcpyAsync(ditems.p, items.data(), sizeof(SaBlockItem) * items.size(), cudaMemcpyHostToDevice, s));
-        if (!tiles.empty()) {
-            sa_pinv_kernel<<<(int) tiles.size(), 256, 0, s>>>(dprobs.p, dtiles.p, d_P, pinv.p, d_err);
-            SLCS_CUDA_TRY(cudaGetLastError());
-        }
-        if (!items.empty()) {
-            sa_block_kernel<<<(int) items.size(), kSaThreads, sizeof(SaShared), s>>>(pinv.p, d_Q, ditems.p, plA.p,
-                                                                                     qlA.p, resA.p, d_err);
-            SLCS_CUDA_TRY(cudaGetLastError());
-        }
-        // problems that fit one block are done
-        for (int i = 0; i < np; ++i)
-            if (n[i] > 0 && n[i] <= kSaSB)
-                SLCS_CUDA_TRY(cudaMemcpyAsync(d_R + off[i], resA.p + off[i], sizeof(int32_t) * n[i],
-                                              cudaMemcpyDeviceToDevice, s));
-        SLCS_CUDA_TRY(cudaStreamSynchronize(s));
-    }
-    if (maxn <= kSaSB) return SLCS_OK;
+    int nprobtiles = 0, nitems = 0;
+    std::vector<int> small;   // problems finished by the shared-memory kernel
+    std::vector<SaLevel> levels;
+    // device
+    SaNode *d_probs = nullptr;
+    SaTile *d_probtiles = nullptr;
+    SaBlockItem *d_items = nullptr;
+    SaNode *d_nodes = nullptr;
+    SaTile *d_tiles = nullptr;
+    int2 *d_tasks = nullptr;
+    int64_t *d_copies = nullptr;
+    int32_t *pinv = nullptr, *pl[2] = {nullptr, nullptr}, *ql[2] = {nullptr, nullptr}, *res[2] = {nullptr, nullptr};
+    int32_t *posP = nullptr, *posQ = nullptr, *xs = nullptr, *ys = nullptr, *tab = nullptr, *vec = nullptr,
+            *cst = nullptr;
+    int64_t tab_max = 0, vec_max = 0, cst_max = 0;
+    cudaStream_t alloc_stream = nullptr;
+    bool shared_scratch = false;   // per-element scratch owned by the caller
+};
 
-    SLCS_TRY(plB.alloc(total, s));
-    SLCS_TRY(qlB.alloc(total, s));
-    SLCS_TRY(resB.alloc(total, s));
-    DevBuf<int32_t> posP, posQ, xs, ys;
-    SLCS_TRY(posP.alloc(total, s));
-    SLCS_TRY(posQ.alloc(total, s));
-    SLCS_TRY(xs.alloc(total, s));
-    SLCS_TRY(ys.alloc(total, s));
-    int32_t *PLc = plA.p, *PLn = plB.p, *QLc = qlA.p, *QLn = qlB.p, *Rc = resA.p, *Rn = resB.p;
-    for (int64_t size = kSaSB; size < maxn; size <<= 1) {
+namespace {
+template <typename T>
+int plan_upload(T **dst, const std::vector<T> &v, cudaStream_t s) {
+    SLCS_TRY(dalloc(reinterpret_cast<void **>(dst), sizeof(T) * std::max<size_t>(v.size(), 1), s));
+    if (!v.empty()) SLCS_CUDA_TRY(cudaMemcpyAsync(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+    return SLCS_OK;
+}
+}  // namespace
+
+// Points a plan created with deferred shared scratch at the caller's buffers.
+int sa_plan_bind(SaPlan *P, const SaScratch *sh) {
+    if (sh->elems < std::max<int64_t>(P->total, 1) || sh->tab < P->tab_max || sh->vec < P->vec_max || sh->cst < P->cst_max)
+        return fail(SLCS_ERR_INTERNAL, "steady-ant shared scratch too small");
+    P->pinv = sh->b[0];
+    P->pl[0] = sh->b[1];
+    P->pl[1] = sh->b[2];
+    P->ql[0] = sh->b[3];
+    P->ql[1] = sh->b[4];
+    P->res[0] = sh->b[5];
+    P->res[1] = sh->b[6];
+    P->posP = sh->b[7];
+    P->posQ = sh->b[8];
+    P->xs = sh->b[9];
+    P->ys = sh->b[10];
+    P->tab = sh->tabp;
+    P->vec = sh->vecp;
+    P->cst = sh->cstp;
+    return SLCS_OK;
+}
+
+void sa_plan_destroy(SaPlan *P) {
+    if (!P) return;
+    cudaStream_t s = P->alloc_stream;
+    void *ptrs[] = {P->d_probs, P->d_probtiles, P->d_items, P->d_nodes, P->d_tiles, P->d_tasks, P->d_copies};
+    for (void *p : ptrs) dfree(p, s);
+    if (!P->shared_scratch) {
+        void *sp[] = {P->pinv, P->pl[0], P->pl[1], P->ql[0], P->ql[1], P->res[0], P->res[1], P->posP, P->posQ,
+                      P->xs, P->ys, P->tab, P->vec, P->cst};
+        for (void *p : sp) dfree(p, s);
+    }
+    delete P;
+}
+
+// Plans the batched unit-Monge products of problems i = 0..np-1, problem i occupying [off[i], off[i] + n[i])
+// of concatenated row->col arrays.  All task lists and scratch are built and allocated here.
+int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, SaPlan **out, cudaStream_t s,
+                   const SaScratch *shared) {
+    *out = nullptr;
+    auto P = new SaPlan();
+    P->alloc_stream = s;
+    P->off = off;
+    P->n = n;
+    P->np = (int) n.size();
+    for (int i = 0; i < P->np; ++i) {
+        P->total = std::max<int64_t>(P->total, off[i] + n[i]);
+        P->maxn = std::max(P->maxn, n[i]);
+    }
+    auto bail = [&](int rc) {
+        sa_plan_destroy(P);
+        return rc;
+    };
+    std::vector<SaNode> probs(P->np);
+    std::vector<SaTile> probtiles;
+    std::vector<SaBlockItem> items;
+    for (int i = 0; i < P->np; ++i) {
+        if (n[i] > 0 && n[i] <= kSaSB) P->small.push_back(i);
+        probs[i] = SaNode{off[i], n[i], n[i], 0, 0, 0, 0, 0};
+        for (int t = 0; (int64_t) t * kMT < n[i]; ++t) probtiles.push_back(SaTile{i, t});
+        for (int b0 = 0; b0 < n[i]; b0 += kSaSB) items.push_back(SaBlockItem{off[i] + b0, std::min(kSaSB, n[i] - b0), 0});
+    }
+    P->nprobtiles = (int) probtiles.size();
+    P->nitems = (int) items.size();
+    std::vector<SaNode> nodes;
+    std::vector<SaTile> tiles;
+    std::vector<int2> tasks;
+    std::vector<int64_t> copies;
+    for (int64_t size = kSaSB; size < P->maxn; size <<= 1) {
         const int64_t span = size << 1;
-        std::vector<SaNode> nodes;
-        std::vector<int64_t> copies;
-        std::vector<int> finished;
-        int64_t tab_tot = 0, vec_tot = 0, cst_tot = 0;
-        for (int i = 0; i < np; ++i) {
-            if (n[i] <= size) continue;   // finished at an earlier level (or in the block kernel)
-            if (n[i] <= span) finished.push_back(i);
+        SaLevel L{};
+        L.size = size;
+        L.o_nodes = (int64_t) nodes.size();
+        L.o_copies = (int64_t) copies.size();
+        const size_t first_node = nodes.size();
+        for (int i = 0; i < P->np; ++i) {
+            if (n[i] <= size) continue;
+            if (n[i] <= span) L.finished.push_back(i);
             for (int64_t a = 0; a < n[i]; a += span) {
                 const int k = (int) std::min<int64_t>(span, n[i] - a);
                 const int h = (int) std::min<int64_t>(size, k);
@@ -652,84 +695,177 @@ int steady_ant_batch_dev(const int32_t *d_P, const int32_t *d_Q, const std::vect
                 int Sc = 256;
                 while ((int64_t) Sc * Sc < k) Sc <<= 1;
                 const int G = (k + Sc - 1) / Sc;
-                SaNode nd{off[i] + a, k, h, Sc, G, tab_tot, vec_tot, cst_tot};
-                tab_tot += (int64_t) (G + 1) * (G + 1);
-                vec_tot += 2 * (int64_t) (G + 1);
-                cst_tot += k / kHSF + 1;
-                nodes.push_back(nd);
+                nodes.push_back(SaNode{off[i] + a, k, h, Sc, G, L.tab_tot, L.vec_tot, L.cst_tot});
+                L.tab_tot += (int64_t) (G + 1) * (G + 1);
+                L.vec_tot += 2 * (int64_t) (G + 1);
+                L.cst_tot += k / kHSF + 1;
             }
         }
-        std::vector<SaTile> tiles;
-        std::vector<int2> lines0, lines1, ctasks, ftasks, wtasks;
-        for (int j = 0; j < (int) nodes.size(); ++j) {
-            const SaNode &nd = nodes[j];
-            for (int t = 0; (int64_t) t * kMT < nd.k; ++t) tiles.push_back(SaTile{j, t});
-            for (int y = 0; y < nd.G + 3; ++y) lines0.push_back(make_int2(j, y));
-            for (int y = 0; y < nd.G + 1; ++y) lines1.push_back(make_int2(j, y));
-            for (int g = 1; g < nd.G; ++g) ctasks.push_back(make_int2(j, g));
+        L.nnodes = (int) (nodes.size() - first_node);
+        L.ncopies = (int) ((copies.size() - L.o_copies) / 2);
+        L.o_tiles = (int64_t) tiles.size();
+        for (int j = 0; j < L.nnodes; ++j)
+            for (int t = 0; (int64_t) t * kMT < nodes[first_node + j].k; ++t) tiles.push_back(SaTile{j, t});
+        L.ntiles = (int) (tiles.size() - L.o_tiles);
+        L.o_l0 = (int64_t) tasks.size();
+        for (int j = 0; j < L.nnodes; ++j)
+            for (int y = 0; y < nodes[first_node + j].G + 3; ++y) tasks.push_back(make_int2(j, y));
+        L.nl0 = (int) (tasks.size() - L.o_l0);
+        L.o_l1 = (int64_t) tasks.size();
+        for (int j = 0; j < L.nnodes; ++j)
+            for (int y = 0; y < nodes[first_node + j].G + 1; ++y) tasks.push_back(make_int2(j, y));
+        L.nl1 = (int) (tasks.size() - L.o_l1);
+        L.o_ct = (int64_t) tasks.size();
+        for (int j = 0; j < L.nnodes; ++j)
+            for (int g = 1; g < nodes[first_node + j].G; ++g) tasks.push_back(make_int2(j, g));
+        L.nct = (int) (tasks.size() - L.o_ct);
+        L.o_ft = (int64_t) tasks.size();
+        for (int j = 0; j < L.nnodes; ++j) {
+            const SaNode &nd = nodes[first_node + j];
             for (int R = kHSF; R < nd.k; R += kHSF)
-                if (R % nd.Sc) ftasks.push_back(make_int2(j, R));
-            for (int top = 0; top < nd.k; top += kHSF) wtasks.push_back(make_int2(j, top));
+                if (R % nd.Sc) tasks.push_back(make_int2(j, R));
         }
-        DevBuf<SaNode> dnodes;
-        DevBuf<SaTile> dtiles;
-        DevBuf<int2> dl0, dl1, dct, dft, dwt;
-        DevBuf<int32_t> tab, vec, cst;
-        DevBuf<int64_t> dcopies;
-        if (!nodes.empty()) {
-            SLCS_TRY(dnodes.alloc(nodes.size(), s));
-            SLCS_TRY(dtiles.alloc(tiles.size(), s));
-            SLCS_TRY(dl0.alloc(lines0.size(), s));
-            SLCS_TRY(dl1.alloc(lines1.size(), s));
-            SLCS_TRY(dct.alloc(std::max<size_t>(ctasks.size(), 1), s));
-            SLCS_TRY(dft.alloc(std::max<size_t>(ftasks.size(), 1), s));
-            SLCS_TRY(dwt.alloc(wtasks.size(), s));
-            SLCS_TRY(tab.alloc(tab_tot, s));
-            SLCS_TRY(vec.alloc(vec_tot, s));
-            SLCS_TRY(cst.alloc(cst_tot, s));
-            SLCS_CUDA_TRY(cudaMemcpyAsync(dnodes.p, nodes.data(), sizeof(SaNode) * nodes.size(), cudaMemcpyHostToDevice, s));
-            SLCS_CUDA_TRY(cudaMemcpyAsync(dtiles.p, tiles.data(), sizeof(SaTile) * tiles.size(), cudaMemcpyHostToDevice, s));
-            SLCS_CUDA_TRY(cudaMemcpyAsync(dl0.p, lines0.data(), sizeof(int2) * lines0.size(), cudaMemcpyHostToDevice, s));
-            SLCS_CUDA_TRY(cudaMemcpyAsync(dl1.p, lines1.data(), sizeof(int2) * lines1.size(), cudaMemcpyHostToDevice, s));
-            if (!ctasks.empty())
-                SLCS_CUDA_TRY(cudaMemcpyAsync(dct.p, ctasks.data(), sizeof(int2) * ctasks.size(), cudaMemcpyHostToDevice, s));
-            if (!ftasks.empty())
-                SLCS_CUDA_TRY(cudaMemcpyAsync(dft.p, ftasks.data(), sizeof(int2) * ftasks.size(), cudaMemcpyHostToDevice, s));
-            SLCS_CUDA_TRY(cudaMemcpyAsync(dwt.p, wtasks.data(), sizeof(int2) * wtasks.size(), cudaMemcpyHostToDevice, s));
-            SLCS_CUDA_TRY(cudaMemsetAsync(tab.p, 0, sizeof(int32_t) * tab_tot, s));
-            SLCS_CUDA_TRY(cudaMemsetAsync(vec.p, 0, sizeof(int32_t) * vec_tot, s));
-            const int nt = (int) tiles.size();
-            sa_merge_kernel<<<nt, 256, 0, s>>>(dnodes.p, dtiles.p, PLc, PLn, posP.p);
-            sa_merge_kernel<<<nt, 256, 0, s>>>(dnodes.p, dtiles.p, QLc, QLn, posQ.p);
-            sa_map_kernel<<<nt, 256, 0, s>>>(dnodes.p, dtiles.p, posP.p, posQ.p, Rc, xs.p, ys.p, tab.p, vec.p, d_err);
-            sa_scan_kernel<<<(int) lines0.size(), 256, 0, s>>>(dnodes.p, dl0.p, tab.p, vec.p, 0);
-            sa_scan_kernel<<<(int) lines1.size(), 256, 0, s>>>(dnodes.p, dl1.p, tab.p, vec.p, 1);
-            if (!ctasks.empty())
-                sa_coarse_kernel<<<(int) ((ctasks.size() + 7) / 8), 256, 0, s>>>(dnodes.p, dct.p, (int) ctasks.size(),
-                                                                                  tab.p, vec.p, ys.p, cst.p);
-            if (!ftasks.empty())
-                sa_fine_kernel<<<(int) ((ftasks.size() + 7) / 8), 256, 0, s>>>(dnodes.p, dft.p, (int) ftasks.size(), xs.p,
-                                                                                ys.p, cst.p);
-            sa_walk_kernel<<<(int) ((wtasks.size() + 255) / 256), 256, 0, s>>>(dnodes.p, dwt.p, (int) wtasks.size(),
-                                                                               xs.p, ys.p, cst.p, Rn);
+        L.nft = (int) (tasks.size() - L.o_ft);
+        L.o_wt = (int64_t) tasks.size();
+        for (int j = 0; j < L.nnodes; ++j)
+            for (int top = 0; top < nodes[first_node + j].k; top += kHSF) tasks.push_back(make_int2(j, top));
+        L.nwt = (int) (tasks.size() - L.o_wt);
+        P->tab_max = std::max(P->tab_max, L.tab_tot);
+        P->vec_max = std::max(P->vec_max, L.vec_tot);
+        P->cst_max = std::max(P->cst_max, L.cst_tot);
+        P->levels.push_back(std::move(L));
+    }
+    int rc;
+    if ((rc = plan_upload(&P->d_probs, probs, s)) || (rc = plan_upload(&P->d_probtiles, probtiles, s)) ||
+        (rc = plan_upload(&P->d_items, items, s)) || (rc = plan_upload(&P->d_nodes, nodes, s)) ||
+        (rc = plan_upload(&P->d_tiles, tiles, s)) || (rc = plan_upload(&P->d_tasks, tasks, s)) ||
+        (rc = plan_upload(&P->d_copies, copies, s)))
+        return bail(rc);
+    const int64_t T = std::max<int64_t>(P->total, 1);
+    if (shared) {
+        P->shared_scratch = true;
+        if (shared->elems >= 0 && (rc = sa_plan_bind(P, shared))) return bail(rc);
+    } else {
+        int32_t **bufs1[] = {&P->pinv, &P->pl[0], &P->ql[0], &P->res[0]};
+        for (auto b : bufs1)
+            if ((rc = dalloc(reinterpret_cast<void **>(b), sizeof(int32_t) * T, s))) return bail(rc);
+        if (!P->levels.empty()) {
+            int32_t **bufs2[] = {&P->pl[1], &P->ql[1], &P->res[1], &P->posP, &P->posQ, &P->xs, &P->ys};
+            for (auto b : bufs2)
+                if ((rc = dalloc(reinterpret_cast<void **>(b), sizeof(int32_t) * T, s))) return bail(rc);
+            if ((rc = dalloc(reinterpret_cast<void **>(&P->tab), sizeof(int32_t) * std::max<int64_t>(P->tab_max, 1), s)) ||
+                (rc = dalloc(reinterpret_cast<void **>(&P->vec), sizeof(int32_t) * std::max<int64_t>(P->vec_max, 1), s)) ||
+                (rc = dalloc(reinterpret_cast<void **>(&P->cst), sizeof(int32_t) * std::max<int64_t>(P->cst_max, 1), s)))
+                return bail(rc);
+        }
+    }
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(sa_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int) sizeof(SaShared));
+        if (e != cudaSuccess) return bail(fail(SLCS_ERR_CUDA, "cudaFuncSetAttribute(sa_block_kernel) failed"));
+        attr_set = true;
+    }
+    *out = P;
+    return SLCS_OK;
+}
+
+// Runs a plan: kernels only (no host synchronisation, no allocation), so the sequence can be captured.
+// Runs a plan: kernels only (no host synchronisation, no allocation), so the sequence can be captured.
+// Permutation mode (d_leafP == nullptr): d_P, d_Q are row->col permutations, d_R receives the product.
+// Leaf mode: d_leafP[j] / d_Q[j] give, for common index j of each problem, the (distinct, arbitrary) id of
+// P's row with column j and of Q's column with row j; the roots' sorted id lists go to d_PLout / d_QLout and
+// the product in root-local coordinates (rank of row id -> rank of column id) to d_R.
+int sa_plan_run_ex(SaPlan *P, const int32_t *d_P, const int32_t *d_leafP, const int32_t *d_Q, int32_t *d_R,
+                   int32_t *d_PLout, int32_t *d_QLout, int *d_err, cudaStream_t s) {
+    if (P->total == 0) return SLCS_OK;
+    const int32_t *leafP = d_leafP;
+    if (!leafP) {
+        if (P->nprobtiles) sa_pinv_kernel<<<P->nprobtiles, 256, 0, s>>>(P->d_probs, P->d_probtiles, d_P, P->pinv, d_err);
+        leafP = P->pinv;
+    }
+    if (P->nitems)
+        sa_block_kernel<<<P->nitems, kSaThreads, sizeof(SaShared), s>>>(leafP, d_Q, P->d_items, P->pl[0], P->ql[0],
+                                                                        P->res[0], d_err);
+    SLCS_CUDA_TRY(cudaGetLastError());
+    auto emit_roots = [&](const std::vector<int> &probs, int buf) -> int {
+        // consecutive problems are copied as one range
+        for (size_t x = 0; x < probs.size();) {
+            size_t y = x + 1;
+            while (y < probs.size() && probs[y] == probs[y - 1] + 1 && P->off[probs[y]] == P->off[probs[y - 1]] + P->n[probs[y - 1]]) ++y;
+            const int64_t o = P->off[probs[x]];
+            const int64_t len = P->off[probs[y - 1]] + P->n[probs[y - 1]] - o;
+            SLCS_CUDA_TRY(cudaMemcpyAsync(d_R + o, P->res[buf] + o, sizeof(int32_t) * len, cudaMemcpyDeviceToDevice, s));
+            if (d_PLout)
+                SLCS_CUDA_TRY(cudaMemcpyAsync(d_PLout + o, P->pl[buf] + o, sizeof(int32_t) * len, cudaMemcpyDeviceToDevice, s));
+            if (d_QLout)
+                SLCS_CUDA_TRY(cudaMemcpyAsync(d_QLout + o, P->ql[buf] + o, sizeof(int32_t) * len, cudaMemcpyDeviceToDevice, s));
+            x = y;
+        }
+        return SLCS_OK;
+    };
+    SLCS_TRY(emit_roots(P->small, 0));
+    int cur = 0;
+    for (const SaLevel &L : P->levels) {
+        const int nxt = cur ^ 1;
+        const SaNode *nodes = P->d_nodes + L.o_nodes;
+        if (L.nnodes) {
+            SLCS_CUDA_TRY(cudaMemsetAsync(P->tab, 0, sizeof(int32_t) * L.tab_tot, s));
+            SLCS_CUDA_TRY(cudaMemsetAsync(P->vec, 0, sizeof(int32_t) * L.vec_tot, s));
+            const SaTile *tiles = P->d_tiles + L.o_tiles;
+            sa_merge_kernel<<<L.ntiles, 256, 0, s>>>(nodes, tiles, P->pl[cur], P->pl[nxt], P->posP);
+            sa_merge_kernel<<<L.ntiles, 256, 0, s>>>(nodes, tiles, P->ql[cur], P->ql[nxt], P->posQ);
+            sa_map_kernel<<<L.ntiles, 256, 0, s>>>(nodes, tiles, P->posP, P->posQ, P->res[cur], P->xs, P->ys, P->tab,
+                                                   P->vec, d_err);
+            sa_scan_kernel<<<L.nl0, 256, 0, s>>>(nodes, P->d_tasks + L.o_l0, P->tab, P->vec, 0);
+            sa_scan_kernel<<<L.nl1, 256, 0, s>>>(nodes, P->d_tasks + L.o_l1, P->tab, P->vec, 1);
+            if (L.nct)
+                sa_coarse_kernel<<<(L.nct + 7) / 8, 256, 0, s>>>(nodes, P->d_tasks + L.o_ct, L.nct, P->tab, P->vec,
+                                                                 P->ys, P->cst);
+            if (L.nft)
+                sa_fine_kernel<<<(L.nft + 7) / 8, 256, 0, s>>>(nodes, P->d_tasks + L.o_ft, L.nft, P->xs, P->ys, P->cst);
+            sa_walk_kernel<<<(L.nwt + 255) / 256, 256, 0, s>>>(nodes, P->d_tasks + L.o_wt, L.nwt, P->xs, P->ys, P->cst,
+                                                               P->res[nxt]);
             SLCS_CUDA_TRY(cudaGetLastError());
         }
-        if (!copies.empty()) {
-            SLCS_TRY(dcopies.alloc(copies.size(), s));
-            SLCS_CUDA_TRY(cudaMemcpyAsync(dcopies.p, copies.data(), sizeof(int64_t) * copies.size(), cudaMemcpyHostToDevice, s));
-            dim3 grid(64, (unsigned) std::min<size_t>(copies.size() / 2, 65535));
-            sa_copy_kernel<<<grid, 256, 0, s>>>(dcopies.p, (int) (copies.size() / 2), PLc, QLc, Rc, PLn, QLn, Rn);
+        if (L.ncopies) {
+            dim3 grid(64, (unsigned) std::min(L.ncopies, 65535));
+            sa_copy_kernel<<<grid, 256, 0, s>>>(P->d_copies + L.o_copies, L.ncopies, P->pl[cur], P->ql[cur],
+                                                P->res[cur], P->pl[nxt], P->ql[nxt], P->res[nxt]);
             SLCS_CUDA_TRY(cudaGetLastError());
         }
-        for (int i : finished)
-            SLCS_CUDA_TRY(cudaMemcpyAsync(d_R + off[i], Rn + off[i], sizeof(int32_t) * n[i], cudaMemcpyDeviceToDevice, s));
-        // the per-level task arrays are freed (stream-ordered) at the end of this scope
-        std::swap(PLc, PLn);
-        std::swap(QLc, QLn);
-        std::swap(Rc, Rn);
-        SLCS_CUDA_TRY(cudaStreamSynchronize(s));
+        SLCS_TRY(emit_roots(L.finished, nxt));
+        cur = nxt;
     }
     return SLCS_OK;
+}
+
+int sa_plan_run(SaPlan *P, const int32_t *d_P, const int32_t *d_Q, int32_t *d_R, int *d_err, cudaStream_t s) {
+    return sa_plan_run_ex(P, d_P, nullptr, d_Q, d_R, nullptr, nullptr, d_err, s);
+}
+
+int sa_plan_launches(const SaPlan *P) {
+    int c = (P->nprobtiles ? 1 : 0) + (P->nitems ? 1 : 0);
+    for (const SaLevel &L : P->levels) c += (L.nnodes ? 6 + (L.nct ? 1 : 0) + (L.nft ? 1 : 0) : 0) + (L.ncopies ? 1 : 0);
+    return c;
+}
+
+int64_t sa_plan_total(const SaPlan *P) { return P->total; }
+
+void sa_plan_needs(const SaPlan *P, int64_t *elems, int64_t *tab, int64_t *vec, int64_t *cst) {
+    *elems = std::max<int64_t>(P->total, 1);
+    *tab = P->tab_max;
+    *vec = P->vec_max;
+    *cst = P->cst_max;
+}
+
+int steady_ant_batch_dev(const int32_t *d_P, const int32_t *d_Q, const std::vector<int64_t> &off,
+                         const std::vector<int> &n, int32_t *d_R, int *d_err, cudaStream_t s) {
+    SaPlan *P = nullptr;
+    SLCS_TRY(sa_plan_create(off, n, &P, s, nullptr));
+    int rc = sa_plan_run(P, d_P, d_Q, d_R, d_err, s);
+    sa_plan_destroy(P);
+    return rc;
 }
 
 int steady_ant_max_small() { return kSaSB; }
@@ -755,6 +891,95 @@ int slcs_steady_ant_dev(const int32_t *d_p, const int32_t *d_q, int n, int32_t *
     SLCS_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(int), s));
     SLCS_TRY(steady_ant_batch_dev(d_p, d_q, std::vector<int64_t>{0}, std::vector<int>{n}, d_r, err.p, s));
     return check_dev_err(err.p, s);
+}
+
+struct slcs_sa_plan {
+    SaPlan *plan = nullptr;
+    int *d_err = nullptr;
+    int device = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    const void *gp = nullptr, *gq = nullptr, *gr = nullptr;
+};
+
+int slcs_sa_plan_create(int n, slcs_sa_plan **out) {
+    if (!out || n < 0 || n >= (1 << 30)) return fail(SLCS_ERR_ARG, "bad plan arguments");
+    *out = nullptr;
+    Engine *E;
+    SLCS_TRY(engine(&E));
+    auto h = new slcs_sa_plan();
+    h->device = E->device;
+    int rc = sa_plan_create(std::vector<int64_t>{0}, std::vector<int>{n}, &h->plan, E->stream, nullptr);
+    if (rc == SLCS_OK) rc = dalloc(reinterpret_cast<void **>(&h->d_err), sizeof(int), E->stream);
+    if (rc == SLCS_OK && cudaMemsetAsync(h->d_err, 0, sizeof(int), E->stream) != cudaSuccess) rc = SLCS_ERR_CUDA;
+    if (rc == SLCS_OK && cudaStreamSynchronize(E->stream) != cudaSuccess) rc = fail(SLCS_ERR_CUDA, "plan setup failed");
+    if (rc != SLCS_OK) {
+        slcs_sa_plan_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return SLCS_OK;
+}
+
+int slcs_sa_plan_run(slcs_sa_plan *h, const int32_t *d_p, const int32_t *d_q, int32_t *d_r, int use_graph,
+                     void *stream) {
+    if (!h) return fail(SLCS_ERR_ARG, "NULL plan");
+    SLCS_CUDA_TRY(cudaSetDevice(h->device));
+    Engine *E;
+    SLCS_TRY(engine(&E));
+    cudaStream_t s = stream ? (cudaStream_t) stream : E->stream;
+    if (!use_graph) return sa_plan_run(h->plan, d_p, d_q, d_r, h->d_err, s);
+    if (!h->gexec || h->gp != d_p || h->gq != d_q || h->gr != d_r) {
+        if (h->gexec) cudaGraphExecDestroy(h->gexec);
+        if (h->graph) cudaGraphDestroy(h->graph);
+        h->gexec = nullptr;
+        h->graph = nullptr;
+        cudaStream_t cap;
+        SLCS_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        SLCS_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        const int rc = sa_plan_run(h->plan, d_p, d_q, d_r, h->d_err, cap);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (rc != SLCS_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return rc != SLCS_OK ? rc : fail(SLCS_ERR_CUDA, std::string("capture failed: ") + cudaGetErrorString(e));
+        }
+        h->graph = g;
+        SLCS_CUDA_TRY(cudaGraphInstantiate(&h->gexec, g, 0));
+        h->gp = d_p;
+        h->gq = d_q;
+        h->gr = d_r;
+    }
+    SLCS_CUDA_TRY(cudaGraphLaunch(h->gexec, s));
+    return SLCS_OK;
+}
+
+int slcs_sa_plan_check(slcs_sa_plan *h, void *stream) {
+    if (!h) return fail(SLCS_ERR_ARG, "NULL plan");
+    Engine *E;
+    SLCS_TRY(engine(&E));
+    return check_dev_err(h->d_err, stream ? (cudaStream_t) stream : E->stream);
+}
+
+int slcs_sa_plan_launches(slcs_sa_plan *h, int32_t *launches) {
+    if (!h || !launches) return fail(SLCS_ERR_ARG, "NULL argument");
+    *launches = sa_plan_launches(h->plan);
+    return SLCS_OK;
+}
+
+int slcs_sa_plan_destroy(slcs_sa_plan *h) {
+    if (!h) return SLCS_OK;
+    cudaSetDevice(h->device);
+    Engine *E = nullptr;
+    if (engine(&E) == SLCS_OK) cudaStreamSynchronize(E->stream);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    if (h->plan) sa_plan_destroy(h->plan);
+    if (h->d_err) dfree(h->d_err, E ? E->stream : nullptr);
+    if (E) cudaStreamSynchronize(E->stream);
+    delete h;
+    return SLCS_OK;
 }
 
 int slcs_steady_ant(const int32_t *p, const int32_t *q, int n, int32_t *r, const slcs_opts *opts) {

@@ -1,0 +1,60 @@
+"""GPU hybrid (tiles combed independently, glued by the GPU steady ant) and the staggered glue, against the
+CPU oracle, the reference's golden glue products and the GPU wavefront.  Bar: bit-exact braids."""
+import os
+
+import numpy as np
+import pytest
+
+from semilocal_b200 import gen
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "golden.npz")
+
+
+def _rand(rng, k, alpha):
+    return rng.integers(0, alpha, k).astype(np.uint8)
+
+
+def test_golden_glues(engine):
+    g = np.load(GOLD)
+    for k in range(int(g["glue_count"])):
+        p, q, out = g[f"glue{k}_p"], g[f"glue{k}_q"], g[f"glue{k}_out"]
+        pm, pn, qm, qn, rg = (int(x) for x in g[f"glue{k}_dims"])
+        assert np.array_equal(engine.staggered_glue(p, pm, pn, q, qm, qn, bool(rg)), out), k
+
+
+def test_glue_vs_oracle(engine, oracle):
+    rng = np.random.default_rng(20)
+    for pm, pn, qm, qn, rg in [(700, 5000, 300, 5000, True), (5000, 700, 5000, 300, False),
+                               (9000, 4500, 100, 4500, True), (33, 9000, 33, 17, False)]:
+        if rg:
+            b = _rand(rng, pn, 4)
+            p = oracle.comb_antidiag(_rand(rng, pm, 4), b, 4)
+            q = oracle.comb_antidiag(_rand(rng, qm, 4), b, 4)
+        else:
+            a = _rand(rng, pm, 4)
+            p = oracle.comb_antidiag(a, _rand(rng, pn, 4), 4)
+            q = oracle.comb_antidiag(a, _rand(rng, qn, 4), 4)
+        assert np.array_equal(engine.staggered_glue(p, pm, pn, q, qm, qn, rg),
+                              oracle.staggered(p, pm, pn, q, qm, qn, rg)), (pm, pn, qm, qn, rg)
+
+
+@pytest.mark.parametrize("m,n,tile", [(1, 1, 1), (1, 50, 8), (50, 1, 8), (37, 41, 8), (300, 200, 64),
+                                      (1000, 1300, 100), (1300, 1000, 96), (2000, 64, 128), (5000, 7000, 1024),
+                                      (9000, 9000, 4096)])
+def test_hybrid_vs_oracle(engine, oracle, m, n, tile):
+    rng = np.random.default_rng(m * 7 + n)
+    a, b = _rand(rng, m, 4), _rand(rng, n, 4)
+    r2c, score = engine.comb(a, b, algo=engine.ALGO_HYBRID, tile=tile)
+    exp = oracle.comb_antidiag(a, b, 8)
+    assert np.array_equal(r2c, exp)
+    assert score == oracle.global_score(exp, m, n)
+
+
+def test_hybrid_equals_wavefront_mutated_pair(engine):
+    """The hybrid-config shape (b mutated from a; 4096 tiles) at 2^16: both GPU paths give one braid."""
+    a, b = gen.hybrid_pair(1 << 16, seed=4)
+    h, sh = engine.comb(a, b, algo=engine.ALGO_HYBRID, tile=4096)
+    w, sw = engine.comb(a, b, algo=engine.ALGO_WAVEFRONT)
+    assert np.array_equal(h, w) and sh == sw
+    assert np.array_equal(np.sort(h), np.arange(len(a) + len(b)))
