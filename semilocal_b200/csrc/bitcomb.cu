@@ -1,0 +1,282 @@
+// bitcomb.cu -- bit-parallel sticky-braid combing (LLCS only) on sm_100a.
+//
+// The reference's bit-parallel combing (R:prefix_lcs/bitwise/transposition_network_binary_alphabet.h:329-411,
+// 668-736) keeps one bit per strand: left strands are 1, top strands 0, and a cell swaps its two strands when
+// the symbols match or a top strand sits in the left slot (the integer rule "swap iff match or left > top",
+// R:include/SemiLocal/SemiLocalLCS.h:158, restricted to the two strand classes).  In bits:
+//     new_top  = left & (top | match)          new_left = top | (left & ~match)
+// and LLCS = m - popcount(final left strands).
+//
+// Layout here: a lane owns strips of 32 rows; a strip's 32 left strands, a-symbol bit planes and the 32 top
+// strands in flight are one 32-bit word each (bit i = row i).  Row i of a strip works on column s - i at
+// step s, so the 32 cells of a step lie on an anti-diagonal and are independent.  Per step:
+//   * (T : IO) is rotated left by one bit: the next input strand enters row 0, the bottom row's output leaves
+//     into IO (2 funnel shifts);
+//   * the b-planes are read as windows "bit i = plane[s - i]" of MSB-first column words (3 funnel shifts:
+//     two symbol bit planes and an "outside the string" plane that turns padding columns into non-matches);
+//   * match and update are 4 three-input logic ops.
+// 9 instructions per 32 cells.  Strips of a lane follow each other one 32-step block apart (the output word
+// of one strip is the input word of the next); lanes are (strips per lane + 1) blocks apart and pass one word
+// per block by shuffle; warps (bands of 32 x RS strips) are chained through a hand-off word array and a
+// progress counter per band, exactly like the integer combing kernel.
+#include <algorithm>
+
+#include "slcs_internal.cuh"
+
+namespace slcs {
+namespace {
+
+struct BitPair {
+    const uint32_t *a1, *a0;        // row planes, word w = rows [32 w, 32 w + 32), bit i = row 32 w + i
+    const uint32_t *b1, *b0, *b2;   // column planes, index q + 1 = columns [32 q, 32 q + 32), MSB first;
+                                    // b2 = 1 outside [0, n); index 0 is a leading pad word
+    uint32_t *hand;                 // hand-off words between bands: word q = columns [32 q, 32 q + 32)
+    int32_t *progress;              // per band: number of hand-off words written
+    int32_t *ones;                  // out: popcount of the final left strands over real rows
+    int m, n, nstrips, nblocks;
+};
+
+struct BitItem {
+    int pair, band, s0, last;
+};
+
+template <int RS>
+__device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int *err, int lane) {
+    uint32_t A1[RS], A0[RS], L[RS], T[RS], V[RS];
+    bool live[RS];
+#pragma unroll
+    for (int r = 0; r < RS; ++r) {
+        const int s = I.s0 + lane * RS + r;
+        live[r] = s < P.nstrips;
+        A1[r] = live[r] ? P.a1[s] : 0u;
+        A0[r] = live[r] ? P.a0[s] : 0u;
+        const int rows = live[r] ? min(32, P.m - 32 * s) : 0;
+        V[r] = rows >= 32 ? 0xffffffffu : ((1u << rows) - 1u);
+        L[r] = 0xffffffffu;
+        T[r] = 0u;
+    }
+    const int nb = P.nblocks;
+    const int delta0 = lane * (RS + 1);
+    const int gmax = 31 * (RS + 1) + RS - 1 + nb;   // iterations until the last strip's last block
+    uint32_t carry = 0u;                            // input word for strip 0 (from the lane above)
+    for (int g = 0; g < gmax; ++g) {
+        // ---- lane 0's input word: from the band above (or zero strands for the first band) ----
+        uint32_t in = carry;
+        int ok = 1;
+        if (lane == 0) {
+            in = 0u;
+            if (I.band > 0 && g < nb) {
+                ok = wait_at_least(P.progress + (I.band - 1), g + 1, err) ? 1 : 0;
+                if (ok) in = __ldcg(P.hand + g);
+            }
+        }
+        if (!__shfl_sync(kFull, ok, 0)) return;   // the bounded wait gave up (error word set)
+#pragma unroll
+        for (int r = 0; r < RS; ++r) {
+            const int q = g - delta0 - r;
+            uint32_t out = 0u;
+            if (live[r] && q >= 0 && q < nb) {
+                uint32_t io = in;
+                const uint32_t h1 = __ldg(P.b1 + q), l1 = __ldg(P.b1 + q + 1);
+                const uint32_t h0 = __ldg(P.b0 + q), l0 = __ldg(P.b0 + q + 1);
+                const uint32_t h2 = __ldg(P.b2 + q), l2 = __ldg(P.b2 + q + 1);
+                uint32_t t = T[r], l = L[r];
+                const uint32_t a1 = A1[r], a0 = A0[r];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const uint32_t nt = __funnelshift_l(io, t, 1);
+                    io = __funnelshift_l(t, io, 1);
+                    const uint32_t w1 = __funnelshift_r(l1, h1, 31 - j);
+                    const uint32_t w0 = __funnelshift_r(l0, h0, 31 - j);
+                    const uint32_t w2 = __funnelshift_r(l2, h2, 31 - j);
+                    const uint32_t y = (a1 ^ w1) | w2;
+                    const uint32_t mt = ~(y | (a0 ^ w0));
+                    t = l & (nt | mt);
+                    l = nt | (l & ~mt);
+                }
+                T[r] = t;
+                L[r] = l;
+                out = io;   // bottom-row outputs of columns [32 (q - 1), 32 q)
+            }
+            in = out;
+        }
+        // ---- the lane's last strip output: to the next lane, and from lane 31 to the band below ----
+        if (lane == 31 && !I.last) {
+            const int q = g - delta0 - (RS - 1);
+            if (q >= 1 && q - 1 < nb) {
+                P.hand[q - 1] = in;
+                __threadfence();
+                st_release(P.progress + I.band, q);
+            }
+        }
+        carry = __shfl_up_sync(kFull, in, 1);
+    }
+    if (!I.last && lane == 31) st_release(P.progress + I.band, nb);
+    int ones = 0;
+#pragma unroll
+    for (int r = 0; r < RS; ++r)
+        if (live[r]) ones += __popc(L[r] & V[r]);
+    ones = __reduce_add_sync(kFull, ones);
+    if (lane == 0 && ones) atomicAdd(P.ones, ones);
+}
+
+template <int RS>
+__global__ void __launch_bounds__(128) bit_kernel(const BitPair *__restrict__ pairs, const BitItem *__restrict__ items,
+                                                  int nitems, int *next, int *err) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int it = nitems;
+        if (lane == 0 && ld_relaxed(err) == kDevErrNone) it = atomicAdd(next, 1);
+        it = __shfl_sync(kFull, it, 0);
+        if (it >= nitems) return;
+        const BitItem I = items[it];
+        bit_band<RS>(pairs[I.pair], I, err, lane);
+    }
+}
+
+// a -> row planes (LSB first per strip); b -> MSB-first column planes with a leading pad word.
+__global__ void bit_pack_kernel(const uint8_t *__restrict__ a, int m, const uint8_t *__restrict__ b, int n,
+                                int nstrips, int nbw, uint32_t *a1, uint32_t *a0, uint32_t *b1, uint32_t *b0,
+                                uint32_t *b2, int *err) {
+    const int lane = threadIdx.x & 31;
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int w = wid; w < nstrips + nbw; w += nwarps) {
+        if (w < nstrips) {
+            const int row = 32 * w + lane;
+            const int sym = row < m ? a[row] : 0;
+            if (sym > 3) raise_error(err, kDevErrBadState);
+            const unsigned h = __ballot_sync(kFull, (sym >> 1) & 1), l = __ballot_sync(kFull, sym & 1);
+            if (lane == 0) {
+                a1[w] = h;
+                a0[w] = l;
+            }
+        } else {
+            const int q = w - nstrips - 1;   // word index q + 1 = w - nstrips
+            const int col = 32 * q + lane;
+            const bool in = q >= 0 && col < n;
+            const int sym = in ? b[col] : 0;
+            if (sym > 3) raise_error(err, kDevErrBadState);
+            const unsigned h = __brev(__ballot_sync(kFull, (sym >> 1) & 1));
+            const unsigned l = __brev(__ballot_sync(kFull, sym & 1));
+            const unsigned o = __brev(__ballot_sync(kFull, !in));
+            if (lane == 0) {
+                b1[w - nstrips] = h;
+                b0[w - nstrips] = l;
+                b2[w - nstrips] = o;
+            }
+        }
+    }
+}
+
+int strips_per_lane(int nstrips) {
+    // four strips per lane (4096 rows per warp) when there are enough rows to keep the device busy
+    if (nstrips >= 4 * 32 * 256) return 4;
+    if (nstrips >= 2 * 32 * 128) return 2;
+    return 1;
+}
+
+}  // namespace
+
+// LLCS of one pair of 2-bit symbol strings on device memory.
+int bitcomb_dev(Engine *E, const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_score, cudaStream_t s) {
+    if (m == 0 || n == 0) {
+        SLCS_CUDA_TRY(cudaMemsetAsync(d_score, 0, sizeof(int32_t), s));
+        return SLCS_OK;
+    }
+    const int nstrips = (m + 31) / 32;
+    const int nblocks = (n + 63) / 32;
+    const int nbw = nblocks + 2;   // column words incl. pads
+    const int RS = strips_per_lane(nstrips);
+    const int per_band = 32 * RS;
+    const int bands = (nstrips + per_band - 1) / per_band;
+    DevBuf<uint32_t> a1, a0, b1, b0, b2, hand;
+    DevBuf<int32_t> prog, ones;
+    DevBuf<int> err, next;
+    DevBuf<BitPair> dp;
+    DevBuf<BitItem> di;
+    SLCS_TRY(a1.alloc(nstrips, s));
+    SLCS_TRY(a0.alloc(nstrips, s));
+    SLCS_TRY(b1.alloc(nbw, s));
+    SLCS_TRY(b0.alloc(nbw, s));
+    SLCS_TRY(b2.alloc(nbw, s));
+    SLCS_TRY(hand.alloc(nblocks + 1, s));
+    SLCS_TRY(prog.alloc(bands, s));
+    SLCS_TRY(ones.alloc(1, s));
+    SLCS_TRY(err.alloc(1, s));
+    SLCS_TRY(next.alloc(1, s));
+    SLCS_TRY(dp.alloc(1, s));
+    SLCS_TRY(di.alloc(bands, s));
+    SLCS_CUDA_TRY(cudaMemsetAsync(prog.p, 0, sizeof(int32_t) * bands, s));
+    SLCS_CUDA_TRY(cudaMemsetAsync(ones.p, 0, sizeof(int32_t), s));
+    SLCS_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+    SLCS_CUDA_TRY(cudaMemsetAsync(next.p, 0, sizeof(int), s));
+    SLCS_CUDA_TRY(cudaMemsetAsync(hand.p, 0, sizeof(uint32_t) * (nblocks + 1), s));
+    BitPair hp{a1.p, a0.p, b1.p, b0.p, b2.p, hand.p, prog.p, ones.p, m, n, nstrips, nblocks};
+    std::vector<BitItem> items(bands);
+    for (int b = 0; b < bands; ++b) items[b] = BitItem{0, b, b * per_band, b == bands - 1 ? 1 : 0};
+    SLCS_CUDA_TRY(cudaMemcpyAsync(dp.p, &hp, sizeof(hp), cudaMemcpyHostToDevice, s));
+    SLCS_CUDA_TRY(cudaMemcpyAsync(di.p, items.data(), sizeof(BitItem) * bands, cudaMemcpyHostToDevice, s));
+    const int pack_warps = nstrips + nbw;
+    bit_pack_kernel<<<std::min(4096, (pack_warps + 7) / 8), 256, 0, s>>>(d_a, m, d_b, n, nstrips, nbw, a1.p, a0.p, b1.p,
+                                                                         b0.p, b2.p, err.p);
+    SLCS_CUDA_TRY(cudaGetLastError());
+    int per_sm = 0;
+    if (RS == 4) SLCS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<4>, 128, 0));
+    else if (RS == 2) SLCS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<2>, 128, 0));
+    else SLCS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<1>, 128, 0));
+    const int warps = std::min(bands, std::max(1, per_sm) * 4 * E->num_sms);
+    const int blocks = (warps + 3) / 4;
+    if (RS == 4) bit_kernel<4><<<blocks, 128, 0, s>>>(dp.p, di.p, bands, next.p, err.p);
+    else if (RS == 2) bit_kernel<2><<<blocks, 128, 0, s>>>(dp.p, di.p, bands, next.p, err.p);
+    else bit_kernel<1><<<blocks, 128, 0, s>>>(dp.p, di.p, bands, next.p, err.p);
+    SLCS_CUDA_TRY(cudaGetLastError());
+    // score = m - ones
+    int32_t h_ones = 0;
+    SLCS_CUDA_TRY(cudaMemcpyAsync(&h_ones, ones.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    SLCS_TRY(check_dev_err(err.p, s));
+    const int32_t score = m - h_ones;
+    SLCS_CUDA_TRY(cudaMemcpyAsync(d_score, &score, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    SLCS_CUDA_TRY(cudaStreamSynchronize(s));
+    return SLCS_OK;
+}
+
+}  // namespace slcs
+
+using namespace slcs;
+
+extern "C" {
+
+int slcs_bitcomb_llcs_u8_dev(const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_score, void *stream) {
+    if (m < 0 || n < 0) return fail(SLCS_ERR_ARG, "negative length");
+    if ((m > 0 && !d_a) || (n > 0 && !d_b) || !d_score) return fail(SLCS_ERR_ARG, "NULL buffer");
+    Engine *E;
+    SLCS_TRY(engine(&E));
+    cudaStream_t s = stream ? (cudaStream_t) stream : E->stream;
+    return bitcomb_dev(E, d_a, m, d_b, n, d_score, s);
+}
+
+int slcs_bitcomb_llcs_u8(const uint8_t *a, int m, const uint8_t *b, int n, int32_t *score) {
+    if (m < 0 || n < 0) return fail(SLCS_ERR_ARG, "negative length");
+    if ((m > 0 && !a) || (n > 0 && !b) || !score) return fail(SLCS_ERR_ARG, "NULL buffer");
+    for (int i = 0; i < m; ++i)
+        if (a[i] > 3) return fail(SLCS_ERR_ARG, "bit-parallel combing needs symbols < 4");
+    for (int i = 0; i < n; ++i)
+        if (b[i] > 3) return fail(SLCS_ERR_ARG, "bit-parallel combing needs symbols < 4");
+    Engine *E;
+    SLCS_TRY(engine(&E));
+    cudaStream_t s = E->stream;
+    DevBuf<uint8_t> da, db;
+    DevBuf<int32_t> ds;
+    SLCS_TRY(da.alloc(m, s));
+    SLCS_TRY(db.alloc(n, s));
+    SLCS_TRY(ds.alloc(1, s));
+    if (m) SLCS_CUDA_TRY(cudaMemcpyAsync(da.p, a, m, cudaMemcpyHostToDevice, s));
+    if (n) SLCS_CUDA_TRY(cudaMemcpyAsync(db.p, b, n, cudaMemcpyHostToDevice, s));
+    SLCS_TRY(bitcomb_dev(E, da.p, m, db.p, n, ds.p, s));
+    SLCS_CUDA_TRY(cudaMemcpyAsync(score, ds.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    SLCS_CUDA_TRY(cudaStreamSynchronize(s));
+    return SLCS_OK;
+}
+
+}  // extern "C"

@@ -4,12 +4,6 @@
 using namespace slcs;
 
 extern "C" {
-int slcs_bitcomb_llcs_u8(const uint8_t *, int, const uint8_t *, int, int32_t *) {
-    return fail(SLCS_ERR_INTERNAL, "bit-parallel kernel not available in this build");
-}
-int slcs_bitcomb_llcs_u8_dev(const uint8_t *, int, const uint8_t *, int, int32_t *, void *) {
-    return fail(SLCS_ERR_INTERNAL, "bit-parallel kernel not available in this build");
-}
 int slcs_scores(const int32_t *, int, int, const slcs_query *, int, int32_t *) {
     return fail(SLCS_ERR_INTERNAL, "score queries not available in this build");
 }
