@@ -299,12 +299,152 @@ def run_ours(args, rank, world, local):
         c_cells, c_s, kind, desc = cpu_reference_batch_sample(pairs, args.cpu_budget, os.cpu_count() or 1)
         result["cpu_baseline"] = {"value": round(c_cells / c_s / 1e9, 3), "unit": "GCUPS",
                                   "cores": os.cpu_count() or 1, "kind": kind, "sample": desc}
+    if rank == 0 and world == 1 and not args.no_suite:
+        result["workloads"] = run_suite(torch, S, peak_cells.value, load_peaks())
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     plan.close()
     if rank == 0:
         print(json.dumps(result), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------------
+# the other workloads (rank 0, N = 1): plain pair, steady ant, hybrid pair -- GPU device-resident timings,
+# parity spot checks, and the reference's CPU path beside each (bounded samples)
+# ------------------------------------------------------------------------------------------------------
+
+def _time_stream(torch, stream, fn, K, W):
+    for _ in range(W):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(K):
+            fn()
+        e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / K
+
+
+def _cpu_time(fn, reps=1):
+    best = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    return best
+
+
+def run_suite(torch, S, peak_cells, peaks):
+    from oracle import oracle as O
+    ncpu = os.cpu_count() or 1
+    use_ref = O.ref_available()
+    st = torch.cuda.Stream()
+    sh = ctypes.c_void_p(st.cuda_stream)
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    out = {}
+
+    # ---- plain pair: a, b uniform over 4 letters, 8192 each; the wavefront on one pair ----
+    a, b = gen.plain_pair(8192, seed=1)
+    m, n = len(a), len(b)
+    da, db = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    r2c = torch.empty(m + n, dtype=torch.int32, device="cuda")
+    sc = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pl = S.PairPlan(m, n, S.ALGO_WAVEFRONT)
+    ms = _time_stream(torch, st, lambda: pl.run(da.data_ptr(), db.data_ptr(), r2c.data_ptr(), sc.data_ptr(), True, sh),
+                      10, 3)
+    pl.check(sh)
+    exp = O.ref_comb(a.astype(np.int32), b.astype(np.int32), "openmp", ncpu) if use_ref else O.comb_antidiag(a, b, ncpu)
+    ok = bool(np.array_equal(r2c.cpu().numpy(), exp))
+    t1 = _cpu_time(lambda: (O.ref_comb(a, b, "openmp", 1) if use_ref else O.comb_antidiag(a, b, 1)), 3)
+    tn = _cpu_time(lambda: (O.ref_comb(a, b, "openmp", ncpu) if use_ref else O.comb_antidiag(a, b, ncpu)), 3)
+    out["plain_pair_8192"] = {
+        "gpu_ms": round(ms, 3), "gcups": round(m * n / ms / 1e6, 1), "bit_exact_vs_cpu": ok,
+        "cpu_ref": {"kind": "reference" if use_ref else "port", "gcups_1t": round(m * n / t1 / 1e9, 2),
+                    "gcups_nt": round(m * n / tn / 1e9, 2), "threads": ncpu,
+                    "impl": "OpenMPIterativeCombing<int,false>"}}
+    pl.close()
+
+    # ---- steady ant: two uniform permutations, n = 2^16 .. 2^24 (headline 2^22) ----
+    sweep = {}
+    for lg in (16, 18, 20, 22, 24):
+        nn = 1 << lg
+        p, q = gen.steady_ant_pair(nn)
+        dp, dq = torch.from_numpy(p).cuda(), torch.from_numpy(q).cuda()
+        dr = torch.empty(nn, dtype=torch.int32, device="cuda")
+        sp = S.SteadyAntPlan(nn)
+        ms = _time_stream(torch, st, lambda: sp.run(dp.data_ptr(), dq.data_ptr(), dr.data_ptr(), True, sh), 5, 3)
+        sp.check(sh)
+        balg = 16 * nn * (max(0, int(np.ceil(np.log2(nn / 4096)))) + 1)
+        ent = {"gpu_ms": round(ms, 3), "gbs_alg": round(balg / ms / 1e6, 1),
+               "hbm_frac": round(balg / ms / 1e6 / hbm_peak, 4), "launches": sp.launches()}
+        if lg == 22:
+            rr = dr.cpu().numpy()
+            if use_ref:
+                O.ref().ref_precalc_warm(5)
+                t0 = time.perf_counter()
+                ref_r = O.ref_braid(p, q, "seq", precalc=5)
+                t_seq = time.perf_counter() - t0
+                t0 = time.perf_counter()
+                O.ref_braid(p, q, "omp", precalc=5, depth=3)
+                t_omp = time.perf_counter() - t0
+            else:
+                t0 = time.perf_counter()
+                ref_r = O.steady_ant(p, q)
+                t_seq = t_omp = time.perf_counter() - t0
+            ent["bit_exact_vs_cpu"] = bool(np.array_equal(rr, ref_r))
+            ent["cpu_ref"] = {"kind": "reference" if use_ref else "port", "seq_s": round(t_seq, 3),
+                              "openmp_depth3_s": round(t_omp, 3), "threads": ncpu,
+                              "impl": "SequentialMemoryOptimizedStickBraidMultiplication / OpenMPStickyBraid(3), "
+                                      "precalc 5"}
+        sweep[str(nn)] = ent
+        sp.close()
+        del dp, dq, dr
+    out["steady_ant"] = sweep
+
+    # ---- hybrid pair: a uniform 2^20, b = a with 5 % subst, 0.5 % ins, 0.5 % del; tiles 4096 ----
+    a, b = gen.hybrid_pair(1 << 20, seed=4)
+    m, n = len(a), len(b)
+    da, db = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    res = {}
+    braids = {}
+    for name, kind in (("hybrid_tiles_4096", S.ALGO_HYBRID), ("wavefront", S.ALGO_WAVEFRONT),
+                       ("bit_parallel", S.PLAN_BITPARALLEL)):
+        pl = S.PairPlan(m, n, kind, tile=4096 if kind == S.ALGO_HYBRID else 0)
+        r2 = torch.empty(m + n, dtype=torch.int32, device="cuda") if kind != S.PLAN_BITPARALLEL else None
+        sc2 = torch.zeros(1, dtype=torch.int32, device="cuda")
+        fn = lambda: pl.run(da.data_ptr(), db.data_ptr(), r2.data_ptr() if r2 is not None else None,
+                            sc2.data_ptr(), True, sh)
+        ms = _time_stream(torch, st, fn, 3, 3)
+        pl.check(sh)
+        kms = pl.kernel_ms()
+        ent = {"gpu_ms": round(ms, 2), "gcups": round(m * n / ms / 1e6, 1), "score": int(sc2.item()),
+               "comb_kernel_ms": round(kms, 2), "launches": pl.launches()}
+        if kind != S.PLAN_BITPARALLEL:
+            ent["int_frac_of_probe"] = round(m * n / (kms * 1e-3) / peak_cells, 4)
+            braids[name] = r2.cpu().numpy()
+        res[name] = ent
+        pl.close()
+    res["hybrid_equals_wavefront"] = bool(np.array_equal(braids["hybrid_tiles_4096"], braids["wavefront"]))
+    res["scores_agree"] = len({res[k]["score"] for k in ("hybrid_tiles_4096", "wavefront", "bit_parallel")}) == 1
+    # the reference's hybrid on a bounded sample: the leading 2^16 x 2^16 corner of the same pair
+    sa, sb = a[:1 << 16].astype(np.int32), b[:1 << 16].astype(np.int32)
+    if use_ref:
+        t = _cpu_time(lambda: O.ref_hybrid_iterative(sa, sb, ncpu, 4096, 4096), 1)
+        tbit_a = a[:1 << 17].astype(np.int32)
+        tbit_b = b[:1 << 17].astype(np.int32)
+        tb = _cpu_time(lambda: O.ref_bit_nary(tbit_a, tbit_b, 4, ncpu), 1)
+        res["cpu_ref"] = {"kind": "reference", "threads": ncpu,
+                          "hybrid_gcups": round(len(sa) * len(sb) / t / 1e9, 2),
+                          "hybrid_sample": "OpenMPHybridIterative<int,false>(threads, 4096, 4096) on the leading "
+                                           "2^16 x 2^16 corner",
+                          "bit_gcups": round(len(tbit_a) * len(tbit_b) / tb / 1e9, 2),
+                          "bit_sample": "llcs_nary_symbol_smart_combing<uint64_t>, 2 bits/symbol, leading 2^17 x 2^17"}
+    out["hybrid_pair_2p20"] = res
+    return out
 
 
 # ------------------------------------------------------------------------------------------------------
@@ -347,6 +487,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work for cpu_baseline")
     ap.add_argument("--ref-step-s", type=float, default=6.0, help="seconds of CPU work per reference step")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-suite", action="store_true", help="skip the plain / steady-ant / hybrid workloads")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -173,6 +173,22 @@ int slcs_batch_kernel_ms(slcs_batch *bt, float *ms);
 int slcs_batch_info(slcs_batch *bt, int64_t *cells, int32_t *launches, int64_t *h2d_bytes, int64_t *d2h_bytes);
 int slcs_batch_destroy(slcs_batch *bt);
 
+/* ---- single-pair plans (device-resident, reusable, graph-capturable) -------------------------- */
+/* kind: SLCS_ALGO_WAVEFRONT, SLCS_ALGO_HYBRID (braid + score) or SLCS_PLAN_BITPARALLEL (score only).
+ * create() plans and allocates everything for an m x n pair; run() launches kernels on `stream` (uint8
+ * device strings; with use_graph != 0 the launch sequence is captured once per buffer set and replayed);
+ * check() waits and reports the device error word; kernel_ms() is the device time of the last run's
+ * combing kernel (CUDA events on the run's stream). */
+#define SLCS_PLAN_BITPARALLEL 3
+typedef struct slcs_pair_plan slcs_pair_plan;
+int slcs_pair_plan_create(int m, int n, int kind, const slcs_opts *opts, slcs_pair_plan **out);
+int slcs_pair_plan_run(slcs_pair_plan *pl, const uint8_t *d_a, const uint8_t *d_b, int32_t *d_row_to_col,
+                       int32_t *d_score, int use_graph, void *stream);
+int slcs_pair_plan_check(slcs_pair_plan *pl, void *stream);
+int slcs_pair_plan_kernel_ms(slcs_pair_plan *pl, float *ms);
+int slcs_pair_plan_launches(slcs_pair_plan *pl, int32_t *launches);
+int slcs_pair_plan_destroy(slcs_pair_plan *pl);
+
 /* ---- measurement helper (no counterpart in the reference) --------------------------------------- */
 /* Issue-rate ceiling of the combing cell's instruction mix on this device, in cells per second
  * (independent cells at full occupancy): the denominator of the combing kernels' roofline fraction. */

@@ -19,6 +19,7 @@ ERRORS = {
 }
 
 ALGO_AUTO, ALGO_WAVEFRONT, ALGO_HYBRID = 0, 1, 2
+PLAN_BITPARALLEL = 3
 Q_GLOBAL, Q_STRING_SUBSTRING, Q_PREFIX_SUFFIX, Q_SUFFIX_PREFIX, Q_SUBSTRING_STRING, Q_MATRIX = range(6)
 
 
@@ -76,6 +77,12 @@ SIGNATURES = {
     "slcs_batch_info": [_vp, _i64p, _i32p, _i64p, _i64p],
     "slcs_batch_destroy": [_vp],
     "slcs_probe_cell_peak": [ctypes.POINTER(ctypes.c_double)],
+    "slcs_pair_plan_create": [_int, _int, _int, _optp, ctypes.POINTER(_vp)],
+    "slcs_pair_plan_run": [_vp, _vp, _vp, _vp, _vp, _int, _vp],
+    "slcs_pair_plan_check": [_vp, _vp],
+    "slcs_pair_plan_kernel_ms": [_vp, ctypes.POINTER(ctypes.c_float)],
+    "slcs_pair_plan_launches": [_vp, _i32p],
+    "slcs_pair_plan_destroy": [_vp],
 }
 
 _lock = threading.Lock()

@@ -234,3 +234,72 @@ def concat_pairs(pairs):
     a_cat = np.ascontiguousarray(np.concatenate([_u8(a) for a, _ in pairs])) if len(pairs) else np.zeros(1, np.uint8)
     b_cat = np.ascontiguousarray(np.concatenate([_u8(b) for _, b in pairs])) if len(pairs) else np.zeros(1, np.uint8)
     return a_cat, a_off, ms, b_cat, b_off, ns
+
+
+class PairPlan:
+    """A reusable single-pair plan on device buffers (include/slcs.h: slcs_pair_plan_*): kind is ALGO_WAVEFRONT,
+    ALGO_HYBRID or PLAN_BITPARALLEL.  run() takes device pointers (ints) and a stream handle."""
+
+    def __init__(self, m: int, n: int, kind: int, tile: int = 0, band_rows: int = 0):
+        o = _lib.opts(kind if kind != _lib.PLAN_BITPARALLEL else 0, tile, tile, band_rows)
+        h = ctypes.c_void_p()
+        check(lib().slcs_pair_plan_create(m, n, kind, ctypes.byref(o), ctypes.byref(h)))
+        self.h, self.m, self.n, self.kind = h, m, n, kind
+
+    def run(self, d_a: int, d_b: int, d_r2c, d_score, use_graph: bool = False, stream=None):
+        check(lib().slcs_pair_plan_run(self.h, d_a, d_b, d_r2c, d_score, int(bool(use_graph)), stream))
+
+    def check(self, stream=None):
+        check(lib().slcs_pair_plan_check(self.h, stream))
+
+    def kernel_ms(self) -> float:
+        v = ctypes.c_float(0)
+        check(lib().slcs_pair_plan_kernel_ms(self.h, ctypes.byref(v)))
+        return float(v.value)
+
+    def launches(self) -> int:
+        v = ctypes.c_int32(0)
+        check(lib().slcs_pair_plan_launches(self.h, ctypes.byref(v)))
+        return int(v.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().slcs_pair_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SteadyAntPlan:
+    """A reusable steady-ant plan of size n (include/slcs.h: slcs_sa_plan_*)."""
+
+    def __init__(self, n: int):
+        h = ctypes.c_void_p()
+        check(lib().slcs_sa_plan_create(n, ctypes.byref(h)))
+        self.h, self.n = h, n
+
+    def run(self, d_p: int, d_q: int, d_r: int, use_graph: bool = False, stream=None):
+        check(lib().slcs_sa_plan_run(self.h, d_p, d_q, d_r, int(bool(use_graph)), stream))
+
+    def check(self, stream=None):
+        check(lib().slcs_sa_plan_check(self.h, stream))
+
+    def launches(self) -> int:
+        v = ctypes.c_int32(0)
+        check(lib().slcs_sa_plan_launches(self.h, ctypes.byref(v)))
+        return int(v.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().slcs_sa_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -176,69 +176,123 @@ int strips_per_lane(int nstrips) {
     return 1;
 }
 
+__global__ void bit_score_kernel(const int32_t *ones, int m, int32_t *score) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *score = m - *ones;
+}
+
 }  // namespace
 
-// LLCS of one pair of 2-bit symbol strings on device memory.
-int bitcomb_dev(Engine *E, const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_score, cudaStream_t s) {
-    if (m == 0 || n == 0) {
+struct BitPlan {
+    int m = 0, n = 0, nstrips = 0, nblocks = 0, nbw = 0, RS = 1, bands = 0, warps = 0;
+    uint32_t *a1 = nullptr, *a0 = nullptr, *b1 = nullptr, *b0 = nullptr, *b2 = nullptr, *hand = nullptr;
+    int32_t *prog = nullptr, *ones = nullptr;
+    int *next = nullptr;
+    BitPair *dp = nullptr;
+    BitItem *di = nullptr;
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+void bit_plan_destroy(BitPlan *B) {
+    if (!B) return;
+    void *ps[] = {B->a1, B->a0, B->b1, B->b0, B->b2, B->hand, B->prog, B->ones, B->next, B->dp, B->di};
+    for (void *p : ps) dfree(p, B->s);
+    if (B->ev0) cudaEventDestroy(B->ev0);
+    if (B->ev1) cudaEventDestroy(B->ev1);
+    delete B;
+}
+
+int bit_plan_create(Engine *E, int m, int n, cudaStream_t s, BitPlan **out) {
+    *out = nullptr;
+    auto B = new BitPlan();
+    B->m = m;
+    B->n = n;
+    B->s = s;
+    B->nstrips = (m + 31) / 32;
+    B->nblocks = (n + 63) / 32;
+    B->nbw = B->nblocks + 2;
+    B->RS = strips_per_lane(B->nstrips);
+    const int per_band = 32 * B->RS;
+    B->bands = std::max(1, (B->nstrips + per_band - 1) / per_band);
+    auto bail = [&](int rc) {
+        bit_plan_destroy(B);
+        return rc;
+    };
+    int rc;
+#define BP_ALLOC(ptr, cnt) \
+    if ((rc = dalloc(reinterpret_cast<void **>(&B->ptr), sizeof(*B->ptr) * std::max<int64_t>((cnt), 1), s))) return bail(rc);
+    BP_ALLOC(a1, B->nstrips);
+    BP_ALLOC(a0, B->nstrips);
+    BP_ALLOC(b1, B->nbw);
+    BP_ALLOC(b0, B->nbw);
+    BP_ALLOC(b2, B->nbw);
+    BP_ALLOC(hand, B->nblocks + 1);
+    BP_ALLOC(prog, B->bands);
+    BP_ALLOC(ones, 1);
+    BP_ALLOC(next, 1);
+    BP_ALLOC(dp, 1);
+    BP_ALLOC(di, B->bands);
+#undef BP_ALLOC
+    BitPair hp{B->a1, B->a0, B->b1, B->b0, B->b2, B->hand, B->prog, B->ones, m, n, B->nstrips, B->nblocks};
+    std::vector<BitItem> items(B->bands);
+    for (int b = 0; b < B->bands; ++b) items[b] = BitItem{0, b, b * per_band, b == B->bands - 1 ? 1 : 0};
+    if (cudaMemcpyAsync(B->dp, &hp, sizeof(hp), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(B->di, items.data(), sizeof(BitItem) * B->bands, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaEventCreate(&B->ev0) != cudaSuccess || cudaEventCreate(&B->ev1) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return bail(fail(SLCS_ERR_CUDA, "bit plan setup failed"));
+    int per_sm = 0;
+    cudaError_t e = B->RS == 4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<4>, 128, 0)
+                  : B->RS == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<2>, 128, 0)
+                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<1>, 128, 0);
+    if (e != cudaSuccess) return bail(fail(SLCS_ERR_CUDA, "occupancy query failed"));
+    B->warps = std::min(B->bands, std::max(1, per_sm) * 4 * E->num_sms);
+    *out = B;
+    return SLCS_OK;
+}
+
+// Kernels only: pack the strings, comb, write the score (device int32) -- capturable.
+int bit_plan_run(BitPlan *B, const uint8_t *d_a, const uint8_t *d_b, int32_t *d_score, int *d_err, cudaStream_t s,
+                 bool capturing) {
+    if (B->m == 0 || B->n == 0) {
         SLCS_CUDA_TRY(cudaMemsetAsync(d_score, 0, sizeof(int32_t), s));
         return SLCS_OK;
     }
-    const int nstrips = (m + 31) / 32;
-    const int nblocks = (n + 63) / 32;
-    const int nbw = nblocks + 2;   // column words incl. pads
-    const int RS = strips_per_lane(nstrips);
-    const int per_band = 32 * RS;
-    const int bands = (nstrips + per_band - 1) / per_band;
-    DevBuf<uint32_t> a1, a0, b1, b0, b2, hand;
-    DevBuf<int32_t> prog, ones;
-    DevBuf<int> err, next;
-    DevBuf<BitPair> dp;
-    DevBuf<BitItem> di;
-    SLCS_TRY(a1.alloc(nstrips, s));
-    SLCS_TRY(a0.alloc(nstrips, s));
-    SLCS_TRY(b1.alloc(nbw, s));
-    SLCS_TRY(b0.alloc(nbw, s));
-    SLCS_TRY(b2.alloc(nbw, s));
-    SLCS_TRY(hand.alloc(nblocks + 1, s));
-    SLCS_TRY(prog.alloc(bands, s));
-    SLCS_TRY(ones.alloc(1, s));
-    SLCS_TRY(err.alloc(1, s));
-    SLCS_TRY(next.alloc(1, s));
-    SLCS_TRY(dp.alloc(1, s));
-    SLCS_TRY(di.alloc(bands, s));
-    SLCS_CUDA_TRY(cudaMemsetAsync(prog.p, 0, sizeof(int32_t) * bands, s));
-    SLCS_CUDA_TRY(cudaMemsetAsync(ones.p, 0, sizeof(int32_t), s));
-    SLCS_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(int), s));
-    SLCS_CUDA_TRY(cudaMemsetAsync(next.p, 0, sizeof(int), s));
-    SLCS_CUDA_TRY(cudaMemsetAsync(hand.p, 0, sizeof(uint32_t) * (nblocks + 1), s));
-    BitPair hp{a1.p, a0.p, b1.p, b0.p, b2.p, hand.p, prog.p, ones.p, m, n, nstrips, nblocks};
-    std::vector<BitItem> items(bands);
-    for (int b = 0; b < bands; ++b) items[b] = BitItem{0, b, b * per_band, b == bands - 1 ? 1 : 0};
-    SLCS_CUDA_TRY(cudaMemcpyAsync(dp.p, &hp, sizeof(hp), cudaMemcpyHostToDevice, s));
-    SLCS_CUDA_TRY(cudaMemcpyAsync(di.p, items.data(), sizeof(BitItem) * bands, cudaMemcpyHostToDevice, s));
-    const int pack_warps = nstrips + nbw;
-    bit_pack_kernel<<<std::min(4096, (pack_warps + 7) / 8), 256, 0, s>>>(d_a, m, d_b, n, nstrips, nbw, a1.p, a0.p, b1.p,
-                                                                         b0.p, b2.p, err.p);
+    SLCS_CUDA_TRY(cudaMemsetAsync(B->prog, 0, sizeof(int32_t) * B->bands, s));
+    SLCS_CUDA_TRY(cudaMemsetAsync(B->ones, 0, sizeof(int32_t), s));
+    SLCS_CUDA_TRY(cudaMemsetAsync(B->next, 0, sizeof(int), s));
+    SLCS_CUDA_TRY(cudaMemsetAsync(B->hand, 0, sizeof(uint32_t) * (B->nblocks + 1), s));
+    const int pack_warps = B->nstrips + B->nbw;
+    bit_pack_kernel<<<std::min(4096, (pack_warps + 7) / 8), 256, 0, s>>>(d_a, B->m, d_b, B->n, B->nstrips, B->nbw, B->a1,
+                                                                         B->a0, B->b1, B->b0, B->b2, d_err);
+    const unsigned fl = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    SLCS_CUDA_TRY(cudaEventRecordWithFlags(B->ev0, s, fl));
+    const int blocks = (B->warps + 3) / 4;
+    if (B->RS == 4) bit_kernel<4><<<blocks, 128, 0, s>>>(B->dp, B->di, B->bands, B->next, d_err);
+    else if (B->RS == 2) bit_kernel<2><<<blocks, 128, 0, s>>>(B->dp, B->di, B->bands, B->next, d_err);
+    else bit_kernel<1><<<blocks, 128, 0, s>>>(B->dp, B->di, B->bands, B->next, d_err);
+    SLCS_CUDA_TRY(cudaEventRecordWithFlags(B->ev1, s, fl));
+    bit_score_kernel<<<1, 32, 0, s>>>(B->ones, B->m, d_score);
     SLCS_CUDA_TRY(cudaGetLastError());
-    int per_sm = 0;
-    if (RS == 4) SLCS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<4>, 128, 0));
-    else if (RS == 2) SLCS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<2>, 128, 0));
-    else SLCS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<1>, 128, 0));
-    const int warps = std::min(bands, std::max(1, per_sm) * 4 * E->num_sms);
-    const int blocks = (warps + 3) / 4;
-    if (RS == 4) bit_kernel<4><<<blocks, 128, 0, s>>>(dp.p, di.p, bands, next.p, err.p);
-    else if (RS == 2) bit_kernel<2><<<blocks, 128, 0, s>>>(dp.p, di.p, bands, next.p, err.p);
-    else bit_kernel<1><<<blocks, 128, 0, s>>>(dp.p, di.p, bands, next.p, err.p);
-    SLCS_CUDA_TRY(cudaGetLastError());
-    // score = m - ones
-    int32_t h_ones = 0;
-    SLCS_CUDA_TRY(cudaMemcpyAsync(&h_ones, ones.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    SLCS_TRY(check_dev_err(err.p, s));
-    const int32_t score = m - h_ones;
-    SLCS_CUDA_TRY(cudaMemcpyAsync(d_score, &score, sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    SLCS_CUDA_TRY(cudaStreamSynchronize(s));
     return SLCS_OK;
+}
+
+int bit_plan_kernel_ms(BitPlan *B, float *ms) {
+    SLCS_CUDA_TRY(cudaEventSynchronize(B->ev1));
+    SLCS_CUDA_TRY(cudaEventElapsedTime(ms, B->ev0, B->ev1));
+    return SLCS_OK;
+}
+
+int bitcomb_dev(Engine *E, const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_score, cudaStream_t s) {
+    BitPlan *B = nullptr;
+    SLCS_TRY(bit_plan_create(E, m, n, s, &B));
+    DevBuf<int> err;
+    int rc = err.alloc(1, s);
+    if (rc == SLCS_OK && cudaMemsetAsync(err.p, 0, sizeof(int), s) != cudaSuccess) rc = fail(SLCS_ERR_CUDA, "memset");
+    if (rc == SLCS_OK) rc = bit_plan_run(B, d_a, d_b, d_score, err.p, s, false);
+    if (rc == SLCS_OK) rc = check_dev_err(err.p, s);
+    bit_plan_destroy(B);
+    return rc;
 }
 
 }  // namespace slcs

@@ -189,10 +189,14 @@ struct HybridPlan {
     cudaStream_t s = nullptr;
     const void *bound_a = nullptr, *bound_b = nullptr;
     std::vector<CombPair> pairs_host;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // around the tile combing launch (optional)
+    bool capturing = false;
 };
 
 void hybrid_plan_destroy(HybridPlan *H) {
     if (!H) return;
+    if (H->ev0) cudaEventDestroy(H->ev0);
+    if (H->ev1) cudaEventDestroy(H->ev1);
     cudaStream_t s = H->s;
     for (GlueLevel &L : H->levels) {
         void *ps[] = {L.d_glues, L.d_carries, L.d_gtiles, L.d_stiles, L.d_ctiles};
@@ -405,7 +409,10 @@ int hybrid_plan_run(HybridPlan *H, const T *d_a, const T *d_b, int *d_err, cudaS
     }
     SLCS_CUDA_TRY(cudaMemsetAsync(H->d_prog, 0, sizeof(int32_t) * std::max(H->nprog, 1), s));
     SLCS_CUDA_TRY(cudaMemsetAsync(H->d_next, 0, sizeof(int), s));
+    const unsigned fl = H->capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    if (H->ev0) SLCS_CUDA_TRY(cudaEventRecordWithFlags(H->ev0, s, fl));
     SLCS_TRY(launch_comb<T>(H->d_pairs, H->d_items, (int) H->items.size(), H->d_next, d_err, H->resident, s));
+    if (H->ev1) SLCS_CUDA_TRY(cudaEventRecordWithFlags(H->ev1, s, fl));
     tiles_invert_kernel<<<(int) H->pairs_host.size(), 256, 0, s>>>(H->c2r[0], H->d_tile_off, H->r2c[0], d_err);
     SLCS_CUDA_TRY(cudaGetLastError());
     int cur = 0;
@@ -441,6 +448,19 @@ int hybrid_score(HybridPlan *H, int32_t *d_score, cudaStream_t s) {
     global_score_kernel<<<std::max(1, std::min(1024, (H->n + 255) / 256)), 256, 0, s>>>(hybrid_result_c2r(H), H->m,
                                                                                         H->n, d_score);
     SLCS_CUDA_TRY(cudaGetLastError());
+    return SLCS_OK;
+}
+
+int hybrid_enable_timing(HybridPlan *H) {
+    if (!H->ev0) SLCS_CUDA_TRY(cudaEventCreate(&H->ev0));
+    if (!H->ev1) SLCS_CUDA_TRY(cudaEventCreate(&H->ev1));
+    return SLCS_OK;
+}
+void hybrid_set_capturing(HybridPlan *H, bool c) { H->capturing = c; }
+int hybrid_comb_ms(HybridPlan *H, float *ms) {
+    if (!H->ev0) return fail(SLCS_ERR_ARG, "timing not enabled");
+    SLCS_CUDA_TRY(cudaEventSynchronize(H->ev1));
+    SLCS_CUDA_TRY(cudaEventElapsedTime(ms, H->ev0, H->ev1));
     return SLCS_OK;
 }
 

@@ -184,5 +184,24 @@ int32_t *hybrid_result_r2c(HybridPlan *H);
 int32_t *hybrid_result_c2r(HybridPlan *H);
 int hybrid_score(HybridPlan *H, int32_t *d_score, cudaStream_t s);
 int hybrid_launches(const HybridPlan *H);
+int hybrid_enable_timing(HybridPlan *H);
+void hybrid_set_capturing(HybridPlan *H, bool c);
+int hybrid_comb_ms(HybridPlan *H, float *ms);
+
+// ------------------------------------------------------------------------------------------------
+// bit-parallel combing (bitcomb.cu)
+// ------------------------------------------------------------------------------------------------
+struct BitPlan;
+int bit_plan_create(Engine *E, int m, int n, cudaStream_t s, BitPlan **out);
+int bit_plan_run(BitPlan *B, const uint8_t *d_a, const uint8_t *d_b, int32_t *d_score, int *d_err, cudaStream_t s,
+                 bool capturing);
+int bit_plan_kernel_ms(BitPlan *B, float *ms);
+void bit_plan_destroy(BitPlan *B);
+
+// ------------------------------------------------------------------------------------------------
+// scores (scores.cu)
+// ------------------------------------------------------------------------------------------------
+int launch_scores(const int32_t *d_r2c, int m, int n, const slcs_query *d_q, int nq, int32_t *d_out, int *d_err,
+                  cudaStream_t s);
 
 }  // namespace slcs
