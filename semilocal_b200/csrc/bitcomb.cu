@@ -9,17 +9,17 @@
 //
 // Layout here: a lane owns strips of 32 rows; a strip's 32 left strands, a-symbol bit planes and the 32 top
 // strands in flight are one 32-bit word each (bit i = row i).  Row i of a strip works on column s - i at
-// step s, so the 32 cells of a step lie on an anti-diagonal and are independent.  Per step:
-//   * (T : IO) is rotated left by one bit: the next input strand enters row 0, the bottom row's output leaves
-//     into IO (2 funnel shifts);
+// step s, so the 32 cells of a step lie on an anti-diagonal and are independent.  Per step and strip:
+//   * T is shifted down one row, the new row-0 strand entering from the strip above (1 funnel shift);
 //   * the b-planes are read as windows "bit i = plane[s - i]" of MSB-first column words (3 funnel shifts:
 //     two symbol bit planes and an "outside the string" plane that turns padding columns into non-matches);
 //   * match and update are 4 three-input logic ops.
-// 9 instructions per 32 cells.  Strips of a lane follow each other one 32-step block apart (the output word
-// of one strip is the input word of the next); lanes are (strips per lane + 1) blocks apart and pass one word
-// per block by shuffle; warps (bands of 32 x RS strips) are chained through a hand-off word array and a
-// progress counter per band, exactly like the integer combing kernel.
+// About 8 instructions per 32 cells.  A lane's strips follow each other one 32-step block apart and update
+// independently; lanes are (strips per lane + 1) blocks apart and pass one word per block by shuffle; warps
+// (bands of 32 x RS strips) are chained through a hand-off word array and a progress counter per band,
+// exactly like the integer combing kernel.
 #include <algorithm>
+#include <cstdlib>
 
 #include "slcs_internal.cuh"
 
@@ -28,8 +28,8 @@ namespace {
 
 struct BitPair {
     const uint32_t *a1, *a0;        // row planes, word w = rows [32 w, 32 w + 32), bit i = row 32 w + i
-    const uint32_t *b1, *b0, *b2;   // column planes, index q + 1 = columns [32 q, 32 q + 32), MSB first;
-                                    // b2 = 1 outside [0, n); index 0 is a leading pad word
+    const uint32_t *b1, *b0, *b2;   // column planes, index q + 2 = columns [32 q, 32 q + 32), MSB first;
+                                    // b2 = 1 outside [0, n); indices 0, 1 are leading pad words
     uint32_t *hand;                 // hand-off words between bands: word q = columns [32 q, 32 q + 32)
     int32_t *progress;              // per band: number of hand-off words written
     int32_t *ones;                  // out: popcount of the final left strands over real rows
@@ -40,6 +40,13 @@ struct BitItem {
     int pair, band, s0, last;
 };
 
+constexpr int kChunk = 16;   // hand-off words between bands are published / polled in groups of kChunk
+
+// One band (warp).  Lane k owns strips s0 + k RS + r, r = 0..RS-1.  The strips of a lane form one systolic
+// chain: strip r works one 32-step block behind strip r-1 and takes its input bit, each step, straight from
+// strip r-1's bottom row (so the RS strips of a lane update independently every step); lanes are RS+1 blocks
+// apart and hand one 32-bit word per block to the next lane by shuffle.  Strips outside their real blocks keep
+// running on padding columns, whose "outside" plane forces non-matches, so the loop has no per-strip branches.
 template <int RS>
 __device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int *err, int lane) {
     uint32_t A1[RS], A0[RS], L[RS], T[RS], V[RS];
@@ -56,60 +63,78 @@ __device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int
         T[r] = 0u;
     }
     const int nb = P.nblocks;
-    const int delta0 = lane * (RS + 1);
-    const int gmax = 31 * (RS + 1) + RS - 1 + nb;   // iterations until the last strip's last block
-    uint32_t carry = 0u;                            // input word for strip 0 (from the lane above)
+    const int lag = lane * (RS + 1);
+    const int gmax = 31 * (RS + 1) + RS - 1 + nb;
+    uint32_t carry = 0u;    // input word of strip 0, from the lane above (previous iteration)
+    uint32_t chunkw = 0u;   // lanes 0..kChunk-1: the current chunk of hand-off words from the band above
+    uint32_t p1[RS], pl1[RS], p0[RS], pl0[RS], p2[RS], pl2[RS];   // plane words of the next iteration
+#pragma unroll
+    for (int r = 0; r < RS; ++r) {
+        const int q = min(max(-lag - r, -1), nb);
+        p1[r] = __ldg(P.b1 + q + 1);
+        pl1[r] = __ldg(P.b1 + q + 2);
+        p0[r] = __ldg(P.b0 + q + 1);
+        pl0[r] = __ldg(P.b0 + q + 2);
+        p2[r] = __ldg(P.b2 + q + 1);
+        pl2[r] = __ldg(P.b2 + q + 2);
+    }
     for (int g = 0; g < gmax; ++g) {
-        // ---- lane 0's input word: from the band above (or zero strands for the first band) ----
-        uint32_t in = carry;
-        int ok = 1;
-        if (lane == 0) {
-            in = 0u;
-            if (I.band > 0 && g < nb) {
-                ok = wait_at_least(P.progress + (I.band - 1), g + 1, err) ? 1 : 0;
-                if (ok) in = __ldcg(P.hand + g);
-            }
+        // lane 0's input word: from the band above (zero strands for the first band).  The band above is
+        // polled once per kChunk words; the chunk's words are then loaded by lanes 0..kChunk-1 in one go and
+        // handed to lane 0 by shuffle, one per iteration.
+        if (I.band > 0 && g < nb && (g % kChunk) == 0) {
+            int ok = 1;
+            if (lane == 0) ok = wait_at_least(P.progress + (I.band - 1), min(nb, g + kChunk), err) ? 1 : 0;
+            if (!__shfl_sync(kFull, ok, 0)) return;   // the bounded wait gave up (error word set)
+            chunkw = (lane < kChunk && g + lane < nb) ? __ldcg(P.hand + g + lane) : 0u;
         }
-        if (!__shfl_sync(kFull, ok, 0)) return;   // the bounded wait gave up (error word set)
+        const uint32_t hw = __shfl_sync(kFull, chunkw, g % kChunk);
+        uint32_t io = lane == 0 ? ((I.band > 0 && g < nb) ? hw : 0u) : carry;
+        // column-plane words of every strip's block (loaded one iteration ahead; q clamped to [-1, nb]:
+        // words q - 1 and q sit at indices q + 1, q + 2 in [0, nb + 2])
+        uint32_t h1[RS], l1[RS], h0[RS], l0[RS], h2[RS], l2[RS];
 #pragma unroll
         for (int r = 0; r < RS; ++r) {
-            const int q = g - delta0 - r;
-            uint32_t out = 0u;
-            if (live[r] && q >= 0 && q < nb) {
-                uint32_t io = in;
-                const uint32_t h1 = __ldg(P.b1 + q), l1 = __ldg(P.b1 + q + 1);
-                const uint32_t h0 = __ldg(P.b0 + q), l0 = __ldg(P.b0 + q + 1);
-                const uint32_t h2 = __ldg(P.b2 + q), l2 = __ldg(P.b2 + q + 1);
-                uint32_t t = T[r], l = L[r];
-                const uint32_t a1 = A1[r], a0 = A0[r];
+            h1[r] = p1[r]; l1[r] = pl1[r]; h0[r] = p0[r]; l0[r] = pl0[r]; h2[r] = p2[r]; l2[r] = pl2[r];
+            const int q = min(max(g + 1 - lag - r, -1), nb);
+            p1[r] = __ldg(P.b1 + q + 1);
+            pl1[r] = __ldg(P.b1 + q + 2);
+            p0[r] = __ldg(P.b0 + q + 1);
+            pl0[r] = __ldg(P.b0 + q + 2);
+            p2[r] = __ldg(P.b2 + q + 1);
+            pl2[r] = __ldg(P.b2 + q + 2);
+        }
+        uint32_t out = 0u;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const uint32_t nt = __funnelshift_l(io, t, 1);
-                    io = __funnelshift_l(t, io, 1);
-                    const uint32_t w1 = __funnelshift_r(l1, h1, 31 - j);
-                    const uint32_t w0 = __funnelshift_r(l0, h0, 31 - j);
-                    const uint32_t w2 = __funnelshift_r(l2, h2, 31 - j);
-                    const uint32_t y = (a1 ^ w1) | w2;
-                    const uint32_t mt = ~(y | (a0 ^ w0));
-                    t = l & (nt | mt);
-                    l = nt | (l & ~mt);
-                }
-                T[r] = t;
-                L[r] = l;
-                out = io;   // bottom-row outputs of columns [32 (q - 1), 32 q)
-            }
-            in = out;
-        }
-        // ---- the lane's last strip output: to the next lane, and from lane 31 to the band below ----
-        if (lane == 31 && !I.last) {
-            const int q = g - delta0 - (RS - 1);
-            if (q >= 1 && q - 1 < nb) {
-                P.hand[q - 1] = in;
-                __threadfence();
-                st_release(P.progress + I.band, q);
+        for (int j = 0; j < 32; ++j) {
+            // rotate every strip's top strands down one row; the new row-0 bit comes from the strip above
+            // (strip 0: the lane's input word), the bottom row of the last strip leaves into `out`
+            uint32_t nt[RS];
+            out = __funnelshift_l(T[RS - 1], out, 1);
+#pragma unroll
+            for (int r = RS - 1; r >= 1; --r) nt[r] = __funnelshift_l(T[r - 1], T[r], 1);
+            nt[0] = __funnelshift_l(io, T[0], 1);
+            io <<= 1;
+#pragma unroll
+            for (int r = 0; r < RS; ++r) {
+                const uint32_t w1 = __funnelshift_r(l1[r], h1[r], 31 - j);
+                const uint32_t w0 = __funnelshift_r(l0[r], h0[r], 31 - j);
+                const uint32_t w2 = __funnelshift_r(l2[r], h2[r], 31 - j);
+                const uint32_t y = (A1[r] ^ w1) | w2;
+                const uint32_t mt = ~(y | (A0[r] ^ w0));
+                const uint32_t l = L[r];
+                T[r] = l & (nt[r] | mt);
+                L[r] = nt[r] | (l & ~mt);
             }
         }
-        carry = __shfl_up_sync(kFull, in, 1);
+        // `out` holds the last strip's bottom-row outputs of its block g - lag - (RS - 1) minus one
+        const int w = g - lag - RS;
+        if (lane == 31 && !I.last && w >= 0 && w < nb) {
+            __stcg(P.hand + w, out);
+            // publish once per kChunk words; the release store orders this lane's earlier stores before it
+            if ((w + 1) % kChunk == 0 || w + 1 == nb) st_release(P.progress + I.band, w + 1);
+        }
+        carry = __shfl_up_sync(kFull, out, 1);
     }
     if (!I.last && lane == 31) st_release(P.progress + I.band, nb);
     int ones = 0;
@@ -121,7 +146,7 @@ __device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int
 }
 
 template <int RS>
-__global__ void __launch_bounds__(128) bit_kernel(const BitPair *__restrict__ pairs, const BitItem *__restrict__ items,
+__global__ void __launch_bounds__(32) bit_kernel(const BitPair *__restrict__ pairs, const BitItem *__restrict__ items,
                                                   int nitems, int *next, int *err) {
     const int lane = threadIdx.x & 31;
     for (;;) {
@@ -134,7 +159,7 @@ __global__ void __launch_bounds__(128) bit_kernel(const BitPair *__restrict__ pa
     }
 }
 
-// a -> row planes (LSB first per strip); b -> MSB-first column planes with a leading pad word.
+// a -> row planes (LSB first per strip); b -> MSB-first column planes with two leading pad words.
 __global__ void bit_pack_kernel(const uint8_t *__restrict__ a, int m, const uint8_t *__restrict__ b, int n,
                                 int nstrips, int nbw, uint32_t *a1, uint32_t *a0, uint32_t *b1, uint32_t *b0,
                                 uint32_t *b2, int *err) {
@@ -152,7 +177,7 @@ __global__ void bit_pack_kernel(const uint8_t *__restrict__ a, int m, const uint
                 a0[w] = l;
             }
         } else {
-            const int q = w - nstrips - 1;   // word index q + 1 = w - nstrips
+            const int q = w - nstrips - 2;   // word index q + 2 = w - nstrips
             const int col = 32 * q + lane;
             const bool in = q >= 0 && col < n;
             const int sym = in ? b[col] : 0;
@@ -170,9 +195,14 @@ __global__ void bit_pack_kernel(const uint8_t *__restrict__ a, int m, const uint
 }
 
 int strips_per_lane(int nstrips) {
-    // four strips per lane (4096 rows per warp) when there are enough rows to keep the device busy
-    if (nstrips >= 4 * 32 * 256) return 4;
-    if (nstrips >= 2 * 32 * 128) return 2;
+    // tuning override (1, 2 or 4 strips of 32 rows per lane), e.g. for the autotuner
+    if (const char *env = getenv("SLCS_BIT_STRIPS_PER_LANE")) {
+        const int v = atoi(env);
+        if (v == 1 || v == 2 || v == 4) return v;
+    }
+    // more strips per lane = fewer bands and more independent work per warp; one pair has only
+    // ~n / (32 * skew) strips in flight, so small values keep more warps busy
+    if (nstrips >= 4 * 32 * 1024) return 2;
     return 1;
 }
 
@@ -210,7 +240,7 @@ int bit_plan_create(Engine *E, int m, int n, cudaStream_t s, BitPlan **out) {
     B->s = s;
     B->nstrips = (m + 31) / 32;
     B->nblocks = (n + 63) / 32;
-    B->nbw = B->nblocks + 2;
+    B->nbw = B->nblocks + 3;   // two leading pads, nblocks words, one trailing pad
     B->RS = strips_per_lane(B->nstrips);
     const int per_band = 32 * B->RS;
     B->bands = std::max(1, (B->nstrips + per_band - 1) / per_band);
@@ -242,11 +272,11 @@ int bit_plan_create(Engine *E, int m, int n, cudaStream_t s, BitPlan **out) {
         cudaStreamSynchronize(s) != cudaSuccess)
         return bail(fail(SLCS_ERR_CUDA, "bit plan setup failed"));
     int per_sm = 0;
-    cudaError_t e = B->RS == 4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<4>, 128, 0)
-                  : B->RS == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<2>, 128, 0)
-                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<1>, 128, 0);
+    cudaError_t e = B->RS == 4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<4>, 32, 0)
+                  : B->RS == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<2>, 32, 0)
+                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bit_kernel<1>, 32, 0);
     if (e != cudaSuccess) return bail(fail(SLCS_ERR_CUDA, "occupancy query failed"));
-    B->warps = std::min(B->bands, std::max(1, per_sm) * 4 * E->num_sms);
+    B->warps = std::min(B->bands, std::max(1, per_sm) * E->num_sms);
     *out = B;
     return SLCS_OK;
 }
@@ -267,10 +297,11 @@ int bit_plan_run(BitPlan *B, const uint8_t *d_a, const uint8_t *d_b, int32_t *d_
                                                                          B->a0, B->b1, B->b0, B->b2, d_err);
     const unsigned fl = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     SLCS_CUDA_TRY(cudaEventRecordWithFlags(B->ev0, s, fl));
-    const int blocks = (B->warps + 3) / 4;
-    if (B->RS == 4) bit_kernel<4><<<blocks, 128, 0, s>>>(B->dp, B->di, B->bands, B->next, d_err);
-    else if (B->RS == 2) bit_kernel<2><<<blocks, 128, 0, s>>>(B->dp, B->di, B->bands, B->next, d_err);
-    else bit_kernel<1><<<blocks, 128, 0, s>>>(B->dp, B->di, B->bands, B->next, d_err);
+    // one warp per block, so that the bands spread over every SM
+    const int blocks = B->warps;
+    if (B->RS == 4) bit_kernel<4><<<blocks, 32, 0, s>>>(B->dp, B->di, B->bands, B->next, d_err);
+    else if (B->RS == 2) bit_kernel<2><<<blocks, 32, 0, s>>>(B->dp, B->di, B->bands, B->next, d_err);
+    else bit_kernel<1><<<blocks, 32, 0, s>>>(B->dp, B->di, B->bands, B->next, d_err);
     SLCS_CUDA_TRY(cudaEventRecordWithFlags(B->ev1, s, fl));
     bit_score_kernel<<<1, 32, 0, s>>>(B->ones, B->m, d_score);
     SLCS_CUDA_TRY(cudaGetLastError());

@@ -115,7 +115,7 @@ __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(128, 3) comb_kernel(const CombPair *__restrict__ pairs,
+__global__ void __launch_bounds__(32, 12) comb_kernel(const CombPair *__restrict__ pairs,
                                                    const CombItem *__restrict__ items, int nitems, int *next,
                                                    int *err) {
     const int lane = threadIdx.x & 31;
@@ -180,9 +180,9 @@ template <typename T>
 int launch_comb(const CombPair *d_pairs, const CombItem *d_items, int nitems, int *d_next, int *d_err,
                 int grid_warps, cudaStream_t s) {
     if (nitems <= 0) return SLCS_OK;
+    // one warp per block (the warps are independent workers), so that few items still spread over all SMs
     const int warps = grid_warps < nitems ? grid_warps : nitems;
-    const int blocks = (warps + 3) / 4;
-    comb_kernel<T><<<blocks, 128, 0, s>>>(d_pairs, d_items, nitems, d_next, d_err);
+    comb_kernel<T><<<warps, 32, 0, s>>>(d_pairs, d_items, nitems, d_next, d_err);
     SLCS_CUDA_TRY(cudaGetLastError());
     return SLCS_OK;
 }
@@ -191,12 +191,12 @@ template int launch_comb<int32_t>(const CombPair *, const CombItem *, int, int *
 
 int comb_resident_warps_sm(int num_sms) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, comb_kernel<uint8_t>, 128, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, comb_kernel<uint8_t>, 32, 0) != cudaSuccess ||
         per_sm <= 0) {
         cudaGetLastError();
-        per_sm = 3;
+        per_sm = 12;
     }
-    return per_sm * 4 * num_sms;
+    return per_sm * num_sms;
 }
 
 int comb_resident_warps(Engine *E) { return comb_resident_warps_sm(E->num_sms); }

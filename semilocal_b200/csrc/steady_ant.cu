@@ -47,7 +47,9 @@ struct SaShared {
     uint16_t posQ[kSaSB];
     uint16_t xs[kSaSB];   // node-local row -> col | hi << 15
     uint16_t ys[kSaSB];   // node-local col -> row | hi << 15
-    int32_t cst[kSaSB / kSaSF + 8];
+    int32_t cst[kSaSB / kSaSF + 8];    // c* at node row R, slot (node start + R) / kSaSF
+    int32_t queue[kSaSB / kSaSF];      // walks left to whole warps
+    int nq;
 };
 
 __device__ __forceinline__ int count_less(const int32_t *arr, int lo, int hi, int32_t v) {
@@ -128,6 +130,39 @@ __device__ __forceinline__ void thread_walk(SaShared &S, int a, int k, int top, 
         const bool good = c >= 1 && c <= k && (hi ? (xr < c) : (xr >= c));
         S.RES[a + r] = (uint16_t) (good ? c - 1 : xr);
     }
+}
+
+constexpr int kWalkSpanMax = 64;   // walks crossing more columns are taken by a whole warp
+
+// one warp: the walk of rows [top, bot) for a walk whose column span is long; rows without a jump are
+// settled 32 at a time by a ballot, every jump is a ballot scan of the columns
+__device__ __forceinline__ void warp_walk(SaShared &S, int a, int k, int top, int bot, int c, int lane) {
+    int rb = bot;   // rows [rb, bot) are done
+    while (rb > top) {
+        const int r = rb - 1 - lane;
+        int v = 0;
+        bool ind = false;
+        if (r >= top) {
+            v = S.xs[a + r];
+            const int x = v & 0x7fff;
+            ind = (v >> 15) ? (x < c) : (x >= c);
+        }
+        const unsigned m = __ballot_sync(kFull, ind);
+        const int j = m ? __ffs(m) - 1 : 32;   // lanes below j keep their point
+        if (lane < j && r >= top) S.RES[a + r] = (uint16_t) (v & 0x7fff);
+        if (j == 32) {
+            rb -= 32;
+            continue;
+        }
+        const int rj = rb - 1 - j;
+        const int vj = __shfl_sync(kFull, v, j);
+        c = warp_col_search(S, a, k, c, 1, rj, lane);
+        const int xr = vj & 0x7fff;
+        const bool good = c >= 1 && c <= k && ((vj >> 15) ? (xr < c) : (xr >= c));
+        if (lane == 0) S.RES[a + rj] = (uint16_t) (good ? c - 1 : xr);
+        rb = rj;
+    }
+    __syncwarp();
 }
 
 __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *__restrict__ Pinv,
@@ -226,26 +261,33 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
                 if (lane == 0) S.cst[(a + R) / kSaSF] = cst;
             }
             __syncthreads();
-            // phase B: fine boundaries (multiples of kSaSF, not of kSaSC), band-restricted scans
-            const int fb_full = (span - 1) / kSaSF;
-            const int fb_last = rem > size ? (rem - 1) / kSaSF : 0;
-            for (int t = warp; t < nfull * fb_full + fb_last; t += nwarps) {
+            // phase B: c* at every multiple of kSaSF (row 0 included) inside each sub-band of min(span, kSaSC)
+            // rows, bottom-up from the boundary below the sub-band
+            const int sb = span < kSaSC ? span : kSaSC;
+            const int sb_full = span / sb;
+            const int sb_last = rem > size ? (rem + sb - 1) / sb : 0;
+            if (tid == 0) S.nq = 0;
+            for (int t = warp; t < nfull * sb_full + sb_last; t += nwarps) {
                 int nd, jj;
-                task_node(t, fb_full, nfull, nd, jj);
+                task_node(t, sb_full, nfull, nd, jj);
                 const int a = nd * span, k = nd < nfull ? span : rem;
-                const int R = (jj + 1) * kSaSF;
-                if (R % kSaSC == 0) continue;
-                const int Rb = min((R / kSaSC + 1) * kSaSC, k);
-                const int cb = Rb >= k ? 0 : S.cst[(a + Rb) / kSaSF];
-                int cst = k + 1;
-                if (cb <= k) {
-                    const int need = warp_row_count(S, a, R, Rb, cb, lane);
-                    cst = warp_col_search(S, a, k, cb, need, R, lane);
+                const int top = jj * sb, bot = min(top + sb, k);
+                int cb = bot >= k ? 0 : S.cst[(a + bot) / kSaSF];
+                const int Rlo = top == 0 ? 0 : top + kSaSF;
+                for (int R = ((bot - 1) / kSaSF) * kSaSF; R >= Rlo; R -= kSaSF) {
+                    const int Rn = min(R + kSaSF, bot);
+                    int cst = k + 1;
+                    if (cb <= k) {
+                        const int need = warp_row_count(S, a, R, Rn, cb, lane);
+                        cst = warp_col_search(S, a, k, cb, need, R, lane);
+                    }
+                    if (lane == 0) S.cst[(a + R) / kSaSF] = cst;
+                    cb = cst;
                 }
-                if (lane == 0) S.cst[(a + R) / kSaSF] = cst;
             }
             __syncthreads();
-            // phase C: walks of kSaSF rows, each from the c* of its bottom boundary
+            // phase C: walks of kSaSF rows, each from the c* of its bottom boundary; long column spans are
+            // queued for whole warps
             const int wb_full = (span + kSaSF - 1) / kSaSF;
             const int wb_last = rem > size ? (rem + kSaSF - 1) / kSaSF : 0;
             for (int t = tid; t < nfull * wb_full + wb_last; t += kSaThreads) {
@@ -254,7 +296,18 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
                 const int a = nd * span, k = nd < nfull ? span : rem;
                 const int top = jj * kSaSF, bot = min(top + kSaSF, k);
                 const int c = bot >= k ? 0 : S.cst[(a + bot) / kSaSF];
-                thread_walk(S, a, k, top, bot, c);
+                const int ce = S.cst[(a + top) / kSaSF];
+                if (min(ce, k) - min(c, k) <= kWalkSpanMax) thread_walk(S, a, k, top, bot, c);
+                else S.queue[atomicAdd(&S.nq, 1)] = t;
+            }
+            __syncthreads();
+            for (int q = warp; q < S.nq; q += nwarps) {
+                const int t = S.queue[q];
+                int nd, jj;
+                task_node(t, wb_full, nfull, nd, jj);
+                const int a = nd * span, k = nd < nfull ? span : rem;
+                const int top = jj * kSaSF, bot = min(top + kSaSF, k);
+                warp_walk(S, a, k, top, bot, bot >= k ? 0 : S.cst[(a + bot) / kSaSF], lane);
             }
         } else {
             for (int node = tid; node < nnodes; node += kSaThreads) {
@@ -276,7 +329,11 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
 // Levels above the shared-memory block: nodes of k > kSaSB common indices, held in global memory.
 // ------------------------------------------------------------------------------------------------------
 constexpr int kMT = 2048;        // merge tile (output elements per CTA)
-constexpr int kHSF = 64;         // rows per walk at HBM levels
+constexpr int kBand = 4096;      // rows per band CTA at HBM levels (a multiple of every coarse block Sc <= 4096)
+constexpr int kBandThreads = 256;
+constexpr int kBandSub = kBand / (kBandThreads / 32);   // rows per warp sub-band
+constexpr int kBandWalk = kBand / kBandThreads;         // rows per thread walk
+constexpr int kBandYCap = 12288;   // columns a band stages in shared memory
 constexpr unsigned kHiBit = 1u << 30;
 constexpr int kValMask = (1 << 30) - 1;
 
@@ -284,11 +341,11 @@ struct SaNode {
     int64_t off;       // first common index of the node
     int k;             // node size
     int h;             // size of the lo child (k - h = hi child)
-    int Sc;            // coarse band (rows/cols per table block), multiple of kHSF
+    int Sc;            // rows/cols per table block (a power of two; divides kBand when Sc <= kBand)
     int G;             // table blocks per dimension: ceil(k / Sc)
     int64_t tab_off;   // offset of the node's (G+1) x (G+1) prefix table
     int64_t vec_off;   // offset of the node's lo-row / lo-col counts (G+1 each)
-    int64_t cst_off;   // offset of the node's c* slots (k / kHSF + 1)
+    int64_t cst_off;   // offset of the node's c* slots, one per band (row b kBand)
 };
 
 struct SaTile {
@@ -454,8 +511,8 @@ __device__ __forceinline__ int hbm_col_search(const int32_t *ys, int64_t off, in
     return k + 1;
 }
 
-// c* at the coarse boundaries R = g Sc (one warp each): the table locates the column block, a ballot scan
-// of at most Sc columns finds the column.
+// c* at the band boundaries R = b kBand that are multiples of Sc (one warp each): the table locates the
+// column block, a ballot scan of at most Sc columns finds the column.
 __global__ void __launch_bounds__(256) sa_coarse_kernel(const SaNode *__restrict__ nodes, const int2 *__restrict__ tasks,
                                                         int ntasks, const int32_t *__restrict__ tab,
                                                         const int32_t *__restrict__ vec, const int32_t *__restrict__ ys,
@@ -463,9 +520,9 @@ __global__ void __launch_bounds__(256) sa_coarse_kernel(const SaNode *__restrict
     const int lane = threadIdx.x & 31;
     const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (t >= ntasks) return;
-    const int2 tk = tasks[t];   // (node, g)
+    const int2 tk = tasks[t];   // (node, band)
     const SaNode nd = nodes[tk.x];
-    const int g = tk.y, R = g * nd.Sc;
+    const int R = tk.y * kBand, g = R / nd.Sc;
     int l = 0, hgh = nd.G + 1;   // first h with delta(R, min(h Sc, k)) >= 0
     while (l < hgh) {
         const int mid = (l + hgh) >> 1;
@@ -479,56 +536,214 @@ __global__ void __launch_bounds__(256) sa_coarse_kernel(const SaNode *__restrict
         const int need = -hbm_delta_corner(nd, tab, vec, g, l - 1);
         c = hbm_col_search(ys, nd.off, nd.k, (l - 1) * nd.Sc, need, R, lane);
     }
-    if (lane == 0) cst[nd.cst_off + R / kHSF] = c;
+    if (lane == 0) cst[nd.cst_off + tk.y] = c;
 }
 
-// c* at the other multiples of kHSF (one warp each), from the coarse boundary below.
+// c* at the band boundaries that are not multiples of Sc (only when Sc > kBand), from the coarse boundary
+// below: delta(R, c) = delta(Rb, c) - #{rows in [R, Rb) whose point raises delta at c}.
 __global__ void __launch_bounds__(256) sa_fine_kernel(const SaNode *__restrict__ nodes, const int2 *__restrict__ tasks,
                                                       int ntasks, const int32_t *__restrict__ xs,
                                                       const int32_t *__restrict__ ys, int32_t *__restrict__ cst) {
     const int lane = threadIdx.x & 31;
     const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (t >= ntasks) return;
-    const int2 tk = tasks[t];   // (node, R)
+    const int2 tk = tasks[t];   // (node, band)
     const SaNode nd = nodes[tk.x];
-    const int R = tk.y;
+    const int R = tk.y * kBand;
     const int Rb = min((R / nd.Sc + 1) * nd.Sc, nd.k);
-    const int cb = Rb >= nd.k ? 0 : cst[nd.cst_off + Rb / kHSF];
+    const int cb = Rb >= nd.k ? 0 : cst[nd.cst_off + Rb / kBand];
     int c = nd.k + 1;
     if (cb <= nd.k) {
         const int need = hbm_row_count(xs, nd.off, R, Rb, cb, lane);
         c = hbm_col_search(ys, nd.off, nd.k, cb, need, R, lane);
     }
-    if (lane == 0) cst[nd.cst_off + R / kHSF] = c;
+    if (lane == 0) cst[nd.cst_off + tk.y] = c;
 }
 
-// Walks of kHSF rows (one thread each) writing the node's product.
-__global__ void __launch_bounds__(256) sa_walk_kernel(const SaNode *__restrict__ nodes, const int2 *__restrict__ tasks,
-                                                      int ntasks, const int32_t *__restrict__ xs,
-                                                      const int32_t *__restrict__ ys, const int32_t *__restrict__ cst,
-                                                      int32_t *__restrict__ RESout) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ntasks) return;
-    const int2 tk = tasks[t];   // (node, top row)
-    const SaNode nd = nodes[tk.x];
-    const int k = nd.k, top = tk.y, bot = min(top + kHSF, k);
-    int c = bot >= k ? 0 : cst[nd.cst_off + bot / kHSF];
-    for (int r = bot - 1; r >= top; --r) {
-        const int v = xs[nd.off + r];
+// ---- band kernel: the ant passage over kBand rows of one node, in shared memory ----
+
+struct BandShared {
+    int32_t x[kBand];                  // the band's rows: col | hi bit, replaced by the product
+    int32_t y[kBandYCap];              // columns [clo, clo + ny): row | hi bit (when they fit)
+    int32_t cst[kBandThreads + 1];     // c* at band rows kBandWalk * j; entry nwalk: the band's bottom
+    int32_t queue[kBandThreads];       // walks left to whole warps
+    int nq;
+};
+
+// Column points of the node: from shared memory when the band's column range was staged, else from global.
+struct YView {
+    const int32_t *s;   // shared copy of columns [clo, clo + ny)
+    const int32_t *g;   // the node's columns in global memory
+    int clo;
+    bool in_smem;
+    __device__ __forceinline__ int operator()(int c) const { return in_smem ? s[c - clo] : __ldg(g + c); }
+};
+
+// warp-wide: rows i in [i0, i1) of the band whose point raises delta when moving up past it at column c
+__device__ __forceinline__ int band_row_count(const int32_t *X, int i0, int i1, int c, int lane) {
+    int total = 0;
+    for (int i = i0; i < i1; i += 32) {
+        const int ii = i + lane;
+        bool q = false;
+        if (ii < i1) {
+            const int v = X[ii];
+            const int x = v & kValMask;
+            q = (v & kHiBit) ? (x < c) : (x >= c);
+        }
+        total += __popc(__ballot_sync(kFull, q));
+    }
+    return total;
+}
+
+// warp-wide: one past the need-th column g in [from, cend) whose point raises delta in row R; k + 1 if none
+__device__ __forceinline__ int band_col_search(const YView &Y, int k, int from, int cend, int need, int R, int lane) {
+    if (need <= 0) return from;
+    for (int g0 = from; g0 < cend; g0 += 32) {
+        const int g = g0 + lane;
+        bool q = false;
+        if (g < cend) {
+            const int w = Y(g);
+            const int y = w & kValMask;
+            q = (w & kHiBit) ? (y < R) : (y >= R);
+        }
+        const unsigned mask = __ballot_sync(kFull, q);
+        const int cnt = __popc(mask);
+        if (need <= cnt) return g0 + (int) __fns(mask, 0, need) + 1;
+        need -= cnt;
+    }
+    return k + 1;
+}
+
+// one thread: band rows [i0, i1) walked up from c = c*(R0 + i1)
+__device__ __forceinline__ void band_thread_walk(int32_t *X, const YView &Y, int k, int R0, int i0, int i1, int c,
+                                                 int cend) {
+    for (int i = i1 - 1; i >= i0; --i) {
+        const int v = X[i];
         const int xr = v & kValMask;
         const bool hi = v & kHiBit;
         if (hi ? (xr < c) : (xr >= c)) {
+            const int r = R0 + i;
             int g = c;
-            for (; g < k; ++g) {
-                const int w = ys[nd.off + g];
+            for (; g < cend; ++g) {
+                const int w = Y(g);
                 const int yr = w & kValMask;
                 if ((w & kHiBit) ? (yr < r) : (yr >= r)) break;
             }
-            c = g < k ? g + 1 : k + 1;
+            c = g < cend ? g + 1 : k + 1;
         }
         const bool good = c >= 1 && c <= k && (hi ? (xr < c) : (xr >= c));
-        RESout[nd.off + r] = good ? c - 1 : xr;
+        X[i] = good ? c - 1 : xr;
     }
+}
+
+// one warp: the same walk for a walk whose columns span is long; rows without a jump are settled 32 at a
+// time by a ballot, every jump is a ballot scan of the columns
+__device__ __forceinline__ void band_warp_walk(int32_t *X, const YView &Y, int k, int R0, int i0, int i1, int c,
+                                               int cend, int lane) {
+    int ib = i1;   // rows [ib, i1) are done
+    while (ib > i0) {
+        const int i = ib - 1 - lane;
+        int v = 0;
+        bool ind = false;
+        if (i >= i0) {
+            v = X[i];
+            const int x = v & kValMask;
+            ind = (v & kHiBit) ? (x < c) : (x >= c);
+        }
+        const unsigned m = __ballot_sync(kFull, ind);
+        const int j = m ? __ffs(m) - 1 : 32;   // lanes below j keep their point
+        if (lane < j && i >= i0) X[i] = v & kValMask;
+        if (j == 32) {
+            ib -= 32;
+            continue;
+        }
+        const int ij = ib - 1 - j;
+        const int vj = __shfl_sync(kFull, v, j);
+        c = band_col_search(Y, k, c, cend, 1, R0 + ij, lane);
+        const int xr = vj & kValMask;
+        const bool good = c >= 1 && c <= k && ((vj & kHiBit) ? (xr < c) : (xr >= c));
+        if (lane == 0) X[ij] = good ? c - 1 : xr;
+        ib = ij;
+    }
+    __syncwarp();
+}
+
+// One CTA per band of kBand rows of a node: c* at every kBandSub rows (scans from the band's bottom), then
+// at every kBandWalk rows (each warp bottom-up through its sub-band), then walks of kBandWalk rows.
+__global__ void __launch_bounds__(kBandThreads) sa_band_kernel(const SaNode *__restrict__ nodes,
+                                                               const int2 *__restrict__ tasks,
+                                                               const int32_t *__restrict__ xs,
+                                                               const int32_t *__restrict__ ys,
+                                                               const int32_t *__restrict__ cst,
+                                                               int32_t *__restrict__ RESout) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BandShared &S = *reinterpret_cast<BandShared *>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int nwarps = kBandThreads / 32;
+    constexpr int wsub = kBandSub / kBandWalk;   // walks per sub-band
+    const int2 tk = tasks[blockIdx.x];   // (node, band)
+    const SaNode nd = nodes[tk.x];
+    const int k = nd.k, R0 = tk.y * kBand, R1 = min(R0 + kBand, k), nr = R1 - R0;
+    const int ctop = cst[nd.cst_off + tk.y];
+    const int cbot = R1 >= k ? 0 : cst[nd.cst_off + tk.y + 1];
+    // columns the band can read: [clo, cend) (c* only grows walking up, and stops at ctop)
+    const int cend = min(ctop, k);
+    const int clo = min(cbot, cend);
+    const int ny = cend - clo;
+    const bool ysm = ny <= kBandYCap;
+    const int nwalk = (nr + kBandWalk - 1) / kBandWalk;
+    for (int i = tid; i < nr; i += kBandThreads) S.x[i] = xs[nd.off + R0 + i];
+    if (ysm)
+        for (int i = tid; i < ny; i += kBandThreads) S.y[i] = ys[nd.off + clo + i];
+    if (tid == 0) {
+        S.cst[0] = ctop;
+        S.cst[nwalk] = cbot;
+        S.nq = 0;
+    }
+    __syncthreads();
+    const YView Y{S.y, ys + nd.off, clo, ysm};
+    // c* at the sub-band tops (warp w >= 1: row R0 + w kBandSub)
+    if (warp >= 1 && warp * kBandSub < nr) {
+        const int i = warp * kBandSub;
+        int c = k + 1;
+        if (cbot <= k) {
+            const int need = band_row_count(S.x, i, nr, cbot, lane);
+            c = band_col_search(Y, k, cbot, cend, need, R0 + i, lane);
+        }
+        if (lane == 0) S.cst[warp * wsub] = c;
+    }
+    __syncthreads();
+    // c* at every walk top inside each sub-band, bottom-up from the boundary below it
+    if (warp * kBandSub < nr) {
+        const int jtop = warp * wsub, jbot = min((warp + 1) * wsub, nwalk);
+        int cb = S.cst[jbot];
+        for (int j = jbot - 1; j > jtop; --j) {
+            const int i = j * kBandWalk, ie = min(i + kBandWalk, nr);
+            int c = k + 1;
+            if (cb <= k) {
+                const int need = band_row_count(S.x, i, ie, cb, lane);
+                c = band_col_search(Y, k, cb, cend, need, R0 + i, lane);
+            }
+            if (lane == 0) S.cst[j] = c;
+            cb = c;
+        }
+    }
+    __syncthreads();
+    // walks: short column spans by one thread each, long ones queued for whole warps
+    if (tid < nwalk) {
+        const int i0 = tid * kBandWalk, i1 = min(i0 + kBandWalk, nr);
+        const int c0 = S.cst[tid + 1], ce = S.cst[tid];
+        if (min(ce, k) - min(c0, k) <= kWalkSpanMax) band_thread_walk(S.x, Y, k, R0, i0, i1, c0, cend);
+        else S.queue[atomicAdd(&S.nq, 1)] = tid;
+    }
+    __syncthreads();
+    for (int q = warp; q < S.nq; q += nwarps) {
+        const int t = S.queue[q];
+        const int i0 = t * kBandWalk, i1 = min(i0 + kBandWalk, nr);
+        band_warp_walk(S.x, Y, k, R0, i0, i1, S.cst[t + 1], cend, lane);
+    }
+    __syncthreads();
+    for (int i = tid; i < nr; i += kBandThreads) RESout[nd.off + R0 + i] = S.x[i];
 }
 
 // Nodes without a sibling at this level carry their lists and product over unchanged.
@@ -698,7 +913,7 @@ int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, S
                 nodes.push_back(SaNode{off[i] + a, k, h, Sc, G, L.tab_tot, L.vec_tot, L.cst_tot});
                 L.tab_tot += (int64_t) (G + 1) * (G + 1);
                 L.vec_tot += 2 * (int64_t) (G + 1);
-                L.cst_tot += k / kHSF + 1;
+                L.cst_tot += (k + kBand - 1) / kBand + 1;
             }
         }
         L.nnodes = (int) (nodes.size() - first_node);
@@ -715,20 +930,24 @@ int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, S
         for (int j = 0; j < L.nnodes; ++j)
             for (int y = 0; y < nodes[first_node + j].G + 1; ++y) tasks.push_back(make_int2(j, y));
         L.nl1 = (int) (tasks.size() - L.o_l1);
+        // band boundaries: from the table where they are multiples of Sc, else from the one below
         L.o_ct = (int64_t) tasks.size();
-        for (int j = 0; j < L.nnodes; ++j)
-            for (int g = 1; g < nodes[first_node + j].G; ++g) tasks.push_back(make_int2(j, g));
+        for (int j = 0; j < L.nnodes; ++j) {
+            const SaNode &nd = nodes[first_node + j];
+            for (int b = 0; (int64_t) b * kBand < nd.k; ++b)
+                if (((int64_t) b * kBand) % nd.Sc == 0) tasks.push_back(make_int2(j, b));
+        }
         L.nct = (int) (tasks.size() - L.o_ct);
         L.o_ft = (int64_t) tasks.size();
         for (int j = 0; j < L.nnodes; ++j) {
             const SaNode &nd = nodes[first_node + j];
-            for (int R = kHSF; R < nd.k; R += kHSF)
-                if (R % nd.Sc) tasks.push_back(make_int2(j, R));
+            for (int b = 0; (int64_t) b * kBand < nd.k; ++b)
+                if (((int64_t) b * kBand) % nd.Sc != 0) tasks.push_back(make_int2(j, b));
         }
         L.nft = (int) (tasks.size() - L.o_ft);
         L.o_wt = (int64_t) tasks.size();
         for (int j = 0; j < L.nnodes; ++j)
-            for (int top = 0; top < nodes[first_node + j].k; top += kHSF) tasks.push_back(make_int2(j, top));
+            for (int b = 0; (int64_t) b * kBand < nodes[first_node + j].k; ++b) tasks.push_back(make_int2(j, b));
         L.nwt = (int) (tasks.size() - L.o_wt);
         P->tab_max = std::max(P->tab_max, L.tab_tot);
         P->vec_max = std::max(P->vec_max, L.vec_tot);
@@ -763,7 +982,9 @@ int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, S
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(sa_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int) sizeof(SaShared));
-        if (e != cudaSuccess) return bail(fail(SLCS_ERR_CUDA, "cudaFuncSetAttribute(sa_block_kernel) failed"));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(sa_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(BandShared));
+        if (e != cudaSuccess) return bail(fail(SLCS_ERR_CUDA, "cudaFuncSetAttribute(steady-ant kernels) failed"));
         attr_set = true;
     }
     *out = P;
@@ -824,8 +1045,8 @@ int sa_plan_run_ex(SaPlan *P, const int32_t *d_P, const int32_t *d_leafP, const 
                                                                  P->ys, P->cst);
             if (L.nft)
                 sa_fine_kernel<<<(L.nft + 7) / 8, 256, 0, s>>>(nodes, P->d_tasks + L.o_ft, L.nft, P->xs, P->ys, P->cst);
-            sa_walk_kernel<<<(L.nwt + 255) / 256, 256, 0, s>>>(nodes, P->d_tasks + L.o_wt, L.nwt, P->xs, P->ys, P->cst,
-                                                               P->res[nxt]);
+            sa_band_kernel<<<L.nwt, kBandThreads, sizeof(BandShared), s>>>(nodes, P->d_tasks + L.o_wt, P->xs, P->ys,
+                                                                           P->cst, P->res[nxt]);
             SLCS_CUDA_TRY(cudaGetLastError());
         }
         if (L.ncopies) {
