@@ -20,6 +20,7 @@
 // delta(r, .).  c* at every 32nd row is found by warp-wide ballot scans; the rows between are walked by one
 // thread each.
 #include <algorithm>
+#include <climits>
 #include <numeric>
 
 #include "slcs_internal.cuh"
@@ -48,9 +49,8 @@ struct SaShared {
     uint16_t xs[kSaSB];   // node-local row -> col | hi << 15
     uint16_t ys[kSaSB];   // node-local col -> row | hi << 15
     int32_t cst[kSaSB / kSaSF + 8];    // c* at node row R, slot (node start + R) / kSaSF
-    int32_t queue[kSaSB / kSaSF];      // walks left to whole warps
-    int nq;
 };
+static_assert(kSaSB / kSaSF <= kSaThreads - 32, "phase C needs at least one warp without a thread walk");
 
 __device__ __forceinline__ int count_less(const int32_t *arr, int lo, int hi, int32_t v) {
     // number of entries < v in the sorted range arr[lo, hi)
@@ -134,6 +134,90 @@ __device__ __forceinline__ void thread_walk(SaShared &S, int a, int k, int top, 
 
 constexpr int kWalkSpanMax = 64;   // walks crossing more columns are taken by a whole warp
 
+// one thread: node-local parent positions of the outputs [d, d + cnt) of the merge of the sorted lists
+// L[a, m) (lo child) and L[m, b) (hi child): a merge-path search for the split of the first d outputs, then a
+// sequential merge (the reference's row / column mappers, R:common/include/Permutations/
+// MongeMultuplicationStrategy.h:208-220, for every element of the two children)
+__device__ __forceinline__ void merge_positions(const int32_t *L, int a, int m, int b, int d, int cnt,
+                                                uint16_t *pos) {
+    const int nlo = m - a, nhi = b - m;
+    int l = max(0, d - nhi), h = min(d, nlo);
+    while (l < h) {
+        const int mid = (l + h) >> 1;
+        if (L[a + mid] < L[m + d - 1 - mid]) l = mid + 1;
+        else h = mid;
+    }
+    int i = l, j = d - l;
+    int32_t vlo = i < nlo ? L[a + i] : INT_MAX;
+    int32_t vhi = j < nhi ? L[m + j] : INT_MAX;
+    for (int s = 0; s < cnt; ++s) {
+        if (vlo < vhi) {
+            pos[a + i] = (uint16_t) (d + s);
+            ++i;
+            vlo = i < nlo ? L[a + i] : INT_MAX;
+        } else {
+            pos[m + j] = (uint16_t) (d + s);
+            ++j;
+            vhi = j < nhi ? L[m + j] : INT_MAX;
+        }
+    }
+}
+
+// one thread: the walk of the kSaSF rows [top, bot) (top a multiple of kSaSF in the block, bot - top <= kSaSF,
+// the rows past bot unused) with the rows' points held in registers and the products written back packed
+__device__ __forceinline__ void thread_walk32(SaShared &S, int a, int k, int top, int bot, int c) {
+    static_assert(kSaSF == 32, "register walk assumes 32-row walks");
+    uint32_t w[16];
+    const uint4 *src = reinterpret_cast<const uint4 *>(S.xs + a + top);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const uint4 u = src[q];
+        w[4 * q] = u.x;
+        w[4 * q + 1] = u.y;
+        w[4 * q + 2] = u.z;
+        w[4 * q + 3] = u.w;
+    }
+    uint32_t o[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) o[q] = 0u;
+    const uint16_t *ys = S.ys + a;
+#pragma unroll
+    for (int i = 31; i >= 0; --i) {
+        const int r = top + i;
+        if (r < bot) {
+            const int v = (int) ((w[i >> 1] >> ((i & 1) * 16)) & 0xffffu);
+            const int xr = v & 0x7fff;
+            const bool hi = v >> 15;
+            if (hi ? (xr < c) : (xr >= c)) {
+                // next column g >= c whose point raises delta in row r; two columns per step
+                int g = c;
+                for (;;) {
+                    if (g >= k) break;
+                    const int w0 = ys[g];
+                    const int w1 = g + 1 < k ? ys[g + 1] : 0;
+                    if ((w0 >> 15) ? ((w0 & 0x7fff) < r) : ((w0 & 0x7fff) >= r)) break;
+                    if (g + 1 >= k) {
+                        g = k;
+                        break;
+                    }
+                    if ((w1 >> 15) ? ((w1 & 0x7fff) < r) : ((w1 & 0x7fff) >= r)) {
+                        g += 1;
+                        break;
+                    }
+                    g += 2;
+                }
+                c = g < k ? g + 1 : k + 1;
+            }
+            const bool good = c >= 1 && c <= k && (hi ? (xr < c) : (xr >= c));
+            o[i >> 1] |= (uint32_t) (good ? c - 1 : xr) << ((i & 1) * 16);
+        }
+    }
+    uint4 *dst = reinterpret_cast<uint4 *>(S.RES + a + top);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) dst[q] = make_uint4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+}
+
+
 // one warp: the walk of rows [top, bot) for a walk whose column span is long; rows without a jump are
 // settled 32 at a time by a ballot, every jump is a ballot scan of the columns
 __device__ __forceinline__ void warp_walk(SaShared &S, int a, int k, int top, int bot, int c, int lane) {
@@ -184,6 +268,21 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
     for (int size = 1; size < nb; size <<= 1) {
         const int span = size << 1;
         // ---- merge the children's lists: positions in the parent lists ----
+        if (span >= 2 * kSaPerThread) {
+            // kSaPerThread consecutive outputs per thread (all inside one node: nodes are aligned multiples)
+            const int o = tid * kSaPerThread;
+            if (o < nb) {
+                const int a = o & ~(span - 1);
+                const int m = min(a + size, nb), b = min(a + span, nb);
+                const int cnt = min(kSaPerThread, b - o);
+                if (m >= b) {
+                    for (int x = 0; x < cnt; ++x) S.posP[o + x] = S.posQ[o + x] = (uint16_t) (o + x - a);
+                } else {
+                    merge_positions(S.PL, a, m, b, o - a, cnt, S.posP);
+                    merge_positions(S.QL, a, m, b, o - a, cnt, S.posQ);
+                }
+            }
+        } else
         for (int e = tid; e < nb; e += kSaThreads) {
             const int a = e & ~(span - 1);
             const int m = min(a + size, nb), b = min(a + span, nb);
@@ -266,7 +365,6 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
             const int sb = span < kSaSC ? span : kSaSC;
             const int sb_full = span / sb;
             const int sb_last = rem > size ? (rem + sb - 1) / sb : 0;
-            if (tid == 0) S.nq = 0;
             for (int t = warp; t < nfull * sb_full + sb_last; t += nwarps) {
                 int nd, jj;
                 task_node(t, sb_full, nfull, nd, jj);
@@ -286,28 +384,55 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
                 }
             }
             __syncthreads();
-            // phase C: walks of kSaSF rows, each from the c* of its bottom boundary; long column spans are
-            // queued for whole warps
-            const int wb_full = (span + kSaSF - 1) / kSaSF;
+            // phase C: walks of kSaSF rows, each from the c* of its bottom boundary.  The first warps walk one
+            // row band per thread; walks with a long column span are left to the remaining warps, which take
+            // them one whole warp each at the same time
+            const int wb_full = span / kSaSF;
             const int wb_last = rem > size ? (rem + kSaSF - 1) / kSaSF : 0;
-            for (int t = tid; t < nfull * wb_full + wb_last; t += kSaThreads) {
+            const int W = nfull * wb_full + wb_last;
+            const int nww = (W + 31) >> 5;
+            auto walk_of = [&](int t, int &a, int &k, int &top, int &bot) {
                 int nd, jj;
                 task_node(t, wb_full, nfull, nd, jj);
-                const int a = nd * span, k = nd < nfull ? span : rem;
-                const int top = jj * kSaSF, bot = min(top + kSaSF, k);
+                a = nd * span;
+                k = nd < nfull ? span : rem;
+                top = jj * kSaSF;
+                bot = min(top + kSaSF, k);
+            };
+            auto is_long = [&](int a, int k, int top, int bot) {
                 const int c = bot >= k ? 0 : S.cst[(a + bot) / kSaSF];
                 const int ce = S.cst[(a + top) / kSaSF];
-                if (min(ce, k) - min(c, k) <= kWalkSpanMax) thread_walk(S, a, k, top, bot, c);
-                else S.queue[atomicAdd(&S.nq, 1)] = t;
-            }
-            __syncthreads();
-            for (int q = warp; q < S.nq; q += nwarps) {
-                const int t = S.queue[q];
-                int nd, jj;
-                task_node(t, wb_full, nfull, nd, jj);
-                const int a = nd * span, k = nd < nfull ? span : rem;
-                const int top = jj * kSaSF, bot = min(top + kSaSF, k);
-                warp_walk(S, a, k, top, bot, bot >= k ? 0 : S.cst[(a + bot) / kSaSF], lane);
+                return min(ce, k) - min(c, k) > kWalkSpanMax;
+            };
+            if (warp < nww) {
+                if (tid < W) {
+                    int a, k, top, bot;
+                    walk_of(tid, a, k, top, bot);
+                    if (!is_long(a, k, top, bot))
+                        thread_walk32(S, a, k, top, bot, bot >= k ? 0 : S.cst[(a + bot) / kSaSF]);
+                }
+            } else {
+                const int h = warp - nww, nh = nwarps - nww;
+                int seen = 0;
+                for (int t0 = 0; t0 < W; t0 += 32) {
+                    bool lng = false;
+                    if (t0 + lane < W) {
+                        int a, k, top, bot;
+                        walk_of(t0 + lane, a, k, top, bot);
+                        lng = is_long(a, k, top, bot);
+                    }
+                    unsigned msk = __ballot_sync(kFull, lng);
+                    while (msk) {
+                        const int l = __ffs(msk) - 1;
+                        msk &= msk - 1;
+                        if (seen % nh == h) {
+                            int a, k, top, bot;
+                            walk_of(t0 + l, a, k, top, bot);
+                            warp_walk(S, a, k, top, bot, bot >= k ? 0 : S.cst[(a + bot) / kSaSF], lane);
+                        }
+                        ++seen;
+                    }
+                }
             }
         } else {
             for (int node = tid; node < nnodes; node += kSaThreads) {
