@@ -189,6 +189,59 @@ int slcs_pair_plan_kernel_ms(slcs_pair_plan *pl, float *ms);
 int slcs_pair_plan_launches(slcs_pair_plan *pl, int32_t *launches);
 int slcs_pair_plan_destroy(slcs_pair_plan *pl);
 
+/* ---- serving loop (no counterpart in the reference) ---------------------------------------------- */
+/* Continuous batching of comparison requests on one GPU.  A request is a pair (a, b) plus one score query
+ * on its braid; the result is what SemiLocalStrategy::compute (R:include/SemiLocal/SemiLocalLCS.h:7-11)
+ * followed by the score readout (R:include/LCS/LCS.h:223-233, R:approximate_matching/utils.h:281-334)
+ * gives.  A worker thread admits requests by a device-memory budget, batches the small ones into
+ * persistent combing launches on several streams (requests at or above big_cells cells run alone on their
+ * own stream), overlaps the launches on the device, and keeps every finished braid resident for further
+ * queries until it is released or evicted (least recently used first) to make room.  Results do not
+ * depend on what else runs. */
+typedef struct slcs_server slcs_server;
+typedef struct slcs_server_opts {
+    int64_t mem_budget;     /* device bytes for in-flight requests and resident braids (0: half the free memory) */
+    int32_t max_pending;    /* submitted but not admitted; beyond it submit returns SLCS_ERR_BUSY (0: 65536) */
+    int32_t small_streams;  /* concurrent batches of small requests (0: 2, at most 16) */
+    int64_t big_cells;      /* m*n at or above which a request runs alone on the big stream (0: 2^32) */
+    int32_t big_warps;      /* persistent-grid cap of a big launch, in warps (0: half the resident warps) */
+    int32_t small_warps;    /* persistent-grid cap of a small batch (0: half the resident warps) */
+    int32_t max_batch;      /* requests per small batch (0: 1024) */
+    int32_t band_rows;      /* rows per band (0: chosen per request) */
+    int32_t reserved[8];
+} slcs_server_opts;
+typedef struct slcs_result {
+    uint64_t ticket;
+    int32_t status;         /* SLCS_OK, or the error that ended the request (SLCS_ERR_BUSY: cancelled) */
+    int32_t score;          /* the query's answer */
+    int32_t m, n;
+    slcs_query query;
+    int32_t pad;
+    double t_submit, t_admit, t_done;   /* seconds on the server's clock (slcs_server_now) */
+} slcs_result;
+typedef struct slcs_server_stats {
+    int64_t submitted, completed, rejected, evicted;
+    int64_t resident, resident_bytes, used_bytes, peak_bytes, budget;
+    int64_t launches, cells;
+    int32_t pending, inflight;
+} slcs_server_stats;
+int slcs_server_create(const slcs_server_opts *opts, slcs_server **out);
+/* Copies a and b (borrowed for the call only); q NULL = global score.  SLCS_ERR_BUSY when the queue is full,
+ * SLCS_ERR_OOM when the request alone exceeds the budget. */
+int slcs_server_submit(slcs_server *srv, const uint8_t *a, int m, const uint8_t *b, int n, const slcs_query *q,
+                       uint64_t *ticket);
+/* Up to cap finished results (waits up to timeout_ms for the first one). */
+int slcs_server_poll(slcs_server *srv, slcs_result *out, int cap, int *count, int timeout_ms);
+/* More queries on a finished request's resident braid (synchronous). */
+int slcs_server_query(slcs_server *srv, uint64_t ticket, const slcs_query *q, int nq, int32_t *out);
+/* Copies a resident braid (row_to_col, m+n entries) to the host. */
+int slcs_server_braid(slcs_server *srv, uint64_t ticket, int32_t *row_to_col);
+int slcs_server_release(slcs_server *srv, uint64_t ticket);
+int slcs_server_stats_get(slcs_server *srv, slcs_server_stats *st);
+double slcs_server_now(slcs_server *srv);
+/* Cancels requests not yet admitted, finishes those on the device, frees everything. */
+int slcs_server_destroy(slcs_server *srv);
+
 /* ---- measurement helper (no counterpart in the reference) --------------------------------------- */
 /* Issue-rate ceiling of the combing cell's instruction mix on this device, in cells per second
  * (independent cells at full occupancy): the denominator of the combing kernels' roofline fraction. */

@@ -38,6 +38,24 @@ class Query(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("i", ctypes.c_int32), ("j", ctypes.c_int32)]
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("mem_budget", ctypes.c_int64), ("max_pending", ctypes.c_int32), ("small_streams", ctypes.c_int32),
+                ("big_cells", ctypes.c_int64), ("big_warps", ctypes.c_int32), ("small_warps", ctypes.c_int32),
+                ("max_batch", ctypes.c_int32), ("band_rows", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("ticket", ctypes.c_uint64), ("status", ctypes.c_int32), ("score", ctypes.c_int32),
+                ("m", ctypes.c_int32), ("n", ctypes.c_int32), ("query", Query), ("pad", ctypes.c_int32),
+                ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in ("submitted", "completed", "rejected", "evicted", "resident",
+                                             "resident_bytes", "used_bytes", "peak_bytes", "budget", "launches",
+                                             "cells")] + [("pending", ctypes.c_int32), ("inflight", ctypes.c_int32)]
+
+
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _i64p = ctypes.POINTER(ctypes.c_int64)
 _u8p = ctypes.POINTER(ctypes.c_uint8)
@@ -83,6 +101,18 @@ SIGNATURES = {
     "slcs_pair_plan_kernel_ms": [_vp, ctypes.POINTER(ctypes.c_float)],
     "slcs_pair_plan_launches": [_vp, _i32p],
     "slcs_pair_plan_destroy": [_vp],
+    "slcs_server_create": [ctypes.POINTER(ServerOpts), ctypes.POINTER(_vp)],
+    "slcs_server_submit": [_vp, _u8p, _int, _u8p, _int, _qp, ctypes.POINTER(ctypes.c_uint64)],
+    "slcs_server_poll": [_vp, ctypes.POINTER(Result), _int, _i32p, _int],
+    "slcs_server_query": [_vp, ctypes.c_uint64, _qp, _int, _i32p],
+    "slcs_server_braid": [_vp, ctypes.c_uint64, _i32p],
+    "slcs_server_release": [_vp, ctypes.c_uint64],
+    "slcs_server_stats_get": [_vp, ctypes.POINTER(ServerStats)],
+    "slcs_server_destroy": [_vp],
+}
+# name -> (argtypes, restype) for entry points that do not return a status
+OTHER_SIGNATURES = {
+    "slcs_server_now": ([_vp], ctypes.c_double),
 }
 
 _lock = threading.Lock()
@@ -117,6 +147,10 @@ def lib() -> ctypes.CDLL:
                 fn = getattr(L, name)
                 fn.argtypes = args
                 fn.restype = ctypes.c_int
+            for name, (args, res) in OTHER_SIGNATURES.items():
+                fn = getattr(L, name)
+                fn.argtypes = args
+                fn.restype = res
             L.slcs_last_error.argtypes = []
             L.slcs_last_error.restype = ctypes.c_char_p
             _lib = L

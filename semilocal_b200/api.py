@@ -303,3 +303,93 @@ class SteadyAntPlan:
             self.close()
         except Exception:
             pass
+
+
+class Server:
+    """Serving loop over the C ABI (slcs_server_*): continuous batching of comparison requests on one GPU.
+
+    submit() copies the pair and returns a ticket at once; a worker thread inside the library admits requests
+    by a device-memory budget, overlaps their launches on the device and keeps finished braids resident;
+    poll() returns finished results.  Results are identical alone and in any mix.
+    """
+
+    def __init__(self, mem_budget: int = 0, small_streams: int = 0, big_cells: int = 0, max_batch: int = 0,
+                 big_warps: int = 0, small_warps: int = 0, band_rows: int = 0, max_pending: int = 0):
+        self._h = ctypes.c_void_p()
+        o = _lib.ServerOpts(mem_budget=mem_budget, max_pending=max_pending, small_streams=small_streams,
+                            big_cells=big_cells, big_warps=big_warps, small_warps=small_warps, max_batch=max_batch,
+                            band_rows=band_rows)
+        _lib.check(_lib.lib().slcs_server_create(ctypes.byref(o), ctypes.byref(self._h)))
+        self._sizes = {}
+
+    def submit(self, a, b, query: Tuple[int, int, int] = (0, 0, 0)) -> int:
+        a, b = _u8(a), _u8(b)
+        t = ctypes.c_uint64()
+        q = _lib.Query(*query)
+        _lib.check(_lib.lib().slcs_server_submit(self._h, _p(a, _u8p), len(a), _p(b, _u8p),
+                                                 len(b), ctypes.byref(q), ctypes.byref(t)))
+        self._sizes[t.value] = (len(a), len(b))
+        return t.value
+
+    def poll(self, cap: int = 1024, timeout_ms: int = 0):
+        buf = (_lib.Result * max(cap, 1))()
+        cnt = ctypes.c_int32()
+        _lib.check(_lib.lib().slcs_server_poll(self._h, buf, cap, ctypes.byref(cnt), timeout_ms))
+        out = []
+        for r in buf[:cnt.value]:
+            out.append({"ticket": r.ticket, "status": r.status, "score": r.score, "m": r.m, "n": r.n,
+                        "query": (r.query.kind, r.query.i, r.query.j), "t_submit": r.t_submit,
+                        "t_admit": r.t_admit, "t_done": r.t_done})
+        return out
+
+    def wait_all(self, tickets, timeout_s: float = 600.0):
+        """Polls until every ticket has a result; returns {ticket: result}."""
+        import time
+        want, got = set(tickets), {}
+        t_end = time.monotonic() + timeout_s
+        while want - set(got):
+            if time.monotonic() > t_end:
+                raise TimeoutError(f"{len(want - set(got))} requests unfinished")
+            for r in self.poll(timeout_ms=50):
+                got[r["ticket"]] = r
+        return got
+
+    def query(self, ticket: int, queries: Sequence[Tuple[int, int, int]]) -> np.ndarray:
+        qs = (_lib.Query * max(len(queries), 1))(*[_lib.Query(*q) for q in queries])
+        out = np.zeros(len(queries), np.int32)
+        _lib.check(_lib.lib().slcs_server_query(self._h, ticket, qs, len(queries), _p(out, _i32p)))
+        return out
+
+    def braid(self, ticket: int) -> np.ndarray:
+        m, n = self._sizes[ticket]
+        out = np.zeros(max(m + n, 1), np.int32)
+        _lib.check(_lib.lib().slcs_server_braid(self._h, ticket, _p(out, _i32p)))
+        return out[:m + n]
+
+    def release(self, ticket: int) -> None:
+        _lib.check(_lib.lib().slcs_server_release(self._h, ticket))
+
+    def stats(self) -> dict:
+        st = _lib.ServerStats()
+        _lib.check(_lib.lib().slcs_server_stats_get(self._h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in _lib.ServerStats._fields_}
+
+    def now(self) -> float:
+        return _lib.lib().slcs_server_now(self._h)
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().slcs_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -13,31 +13,6 @@
 namespace slcs {
 namespace {
 
-__device__ __forceinline__ void query_to_matrix(const slcs_query &q, int m, int n, int &i, int &j, int &offset,
-                                                bool &ok) {
-    ok = true;
-    offset = 0;
-    switch (q.kind) {
-        case SLCS_Q_GLOBAL: i = m; j = n; break;
-        case SLCS_Q_STRING_SUBSTRING:   // LCS(a, b[i..j)) = H(i + m, j)
-            ok = 0 <= q.i && q.i <= q.j && q.j <= n;
-            i = q.i + m; j = q.j; break;
-        case SLCS_Q_PREFIX_SUFFIX:      // LCS(a[0..i), b[j..n)) = H(j + m, n + m - i) - (m - i)
-            ok = 0 <= q.i && q.i <= m && 0 <= q.j && q.j <= n;
-            i = q.j + m; j = n + m - q.i; offset = -(m - q.i); break;
-        case SLCS_Q_SUFFIX_PREFIX:      // LCS(a[i..m), b[0..j)) = H(m - i, j) - i
-            ok = 0 <= q.i && q.i <= m && 0 <= q.j && q.j <= n;
-            i = m - q.i; j = q.j; offset = -q.i; break;
-        case SLCS_Q_SUBSTRING_STRING:   // LCS(a[i..j), b) = H(m - i, n + m - j) - i - (m - j)
-            ok = 0 <= q.i && q.i <= q.j && q.j <= m;
-            i = m - q.i; j = n + m - q.j; offset = -q.i - (m - q.j); break;
-        case SLCS_Q_MATRIX:
-            ok = 0 <= q.i && q.i <= m + n && 0 <= q.j && q.j <= m + n;
-            i = q.i; j = q.j; break;
-        default: ok = false; i = j = 0;
-    }
-}
-
 __global__ void __launch_bounds__(256) scores_kernel(const int32_t *__restrict__ r2c, int m, int n,
                                                      const slcs_query *__restrict__ qs, int nq,
                                                      int32_t *__restrict__ out, int *err) {
@@ -83,6 +58,22 @@ int scores_dev(const int32_t *d_r2c, int m, int n, const slcs_query *d_q, int nq
 int launch_scores(const int32_t *d_r2c, int m, int n, const slcs_query *d_q, int nq, int32_t *d_out, int *d_err,
                   cudaStream_t s) {
     return scores_dev(d_r2c, m, n, d_q, nq, d_out, d_err, s);
+}
+
+int launch_scores_host(const int32_t *d_r2c, int m, int n, const slcs_query *q, int nq, int32_t *out,
+                       cudaStream_t s) {
+    if (nq <= 0) return SLCS_OK;
+    DevBuf<slcs_query> dq;
+    DevBuf<int32_t> dout;
+    DevBuf<int> err;
+    SLCS_TRY(dq.alloc(nq, s));
+    SLCS_TRY(dout.alloc(nq, s));
+    SLCS_TRY(err.alloc(1, s));
+    SLCS_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+    SLCS_CUDA_TRY(cudaMemcpyAsync(dq.p, q, sizeof(slcs_query) * nq, cudaMemcpyHostToDevice, s));
+    SLCS_TRY(scores_dev(d_r2c, m, n, dq.p, nq, dout.p, err.p, s));
+    SLCS_CUDA_TRY(cudaMemcpyAsync(out, dout.p, sizeof(int32_t) * nq, cudaMemcpyDeviceToHost, s));
+    return check_dev_err(err.p, s);
 }
 
 }  // namespace slcs

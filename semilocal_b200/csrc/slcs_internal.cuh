@@ -201,7 +201,38 @@ void bit_plan_destroy(BitPlan *B);
 // ------------------------------------------------------------------------------------------------
 // scores (scores.cu)
 // ------------------------------------------------------------------------------------------------
+// Maps a query to the semi-local matrix entry H(i, j) it reads and the offset added to it; ok = false for
+// arguments out of range.  Semantics: R:include/SemiLocal/SemiLocalLCS.h:13-63, R:approximate_matching/
+// utils.h:281-334.
+__device__ __forceinline__ void query_to_matrix(const slcs_query &q, int m, int n, int &i, int &j, int &offset,
+                                                bool &ok) {
+    ok = true;
+    offset = 0;
+    switch (q.kind) {
+        case SLCS_Q_GLOBAL: i = m; j = n; break;
+        case SLCS_Q_STRING_SUBSTRING:   // LCS(a, b[i..j)) = H(i + m, j)
+            ok = 0 <= q.i && q.i <= q.j && q.j <= n;
+            i = q.i + m; j = q.j; break;
+        case SLCS_Q_PREFIX_SUFFIX:      // LCS(a[0..i), b[j..n)) = H(j + m, n + m - i) - (m - i)
+            ok = 0 <= q.i && q.i <= m && 0 <= q.j && q.j <= n;
+            i = q.j + m; j = n + m - q.i; offset = -(m - q.i); break;
+        case SLCS_Q_SUFFIX_PREFIX:      // LCS(a[i..m), b[0..j)) = H(m - i, j) - i
+            ok = 0 <= q.i && q.i <= m && 0 <= q.j && q.j <= n;
+            i = m - q.i; j = q.j; offset = -q.i; break;
+        case SLCS_Q_SUBSTRING_STRING:   // LCS(a[i..j), b) = H(m - i, n + m - j) - i - (m - j)
+            ok = 0 <= q.i && q.i <= q.j && q.j <= m;
+            i = m - q.i; j = n + m - q.j; offset = -q.i - (m - q.j); break;
+        case SLCS_Q_MATRIX:
+            ok = 0 <= q.i && q.i <= m + n && 0 <= q.j && q.j <= m + n;
+            i = q.i; j = q.j; break;
+        default: ok = false; i = j = 0;
+    }
+}
+
 int launch_scores(const int32_t *d_r2c, int m, int n, const slcs_query *d_q, int nq, int32_t *d_out, int *d_err,
                   cudaStream_t s);
+// The same for host queries / answers (synchronous on s).
+int launch_scores_host(const int32_t *d_r2c, int m, int n, const slcs_query *q, int nq, int32_t *out,
+                       cudaStream_t s);
 
 }  // namespace slcs

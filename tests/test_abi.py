@@ -34,7 +34,8 @@ def test_library_exports_every_declared_symbol():
 def test_python_signatures_cover_header():
     from semilocal_b200 import _lib
     names = set(declared_functions()) - {"slcs_last_error"}
-    assert names <= set(_lib.SIGNATURES), sorted(names - set(_lib.SIGNATURES))
+    covered = set(_lib.SIGNATURES) | set(_lib.OTHER_SIGNATURES)
+    assert names <= covered, sorted(names - covered)
 
 
 def test_no_device_fails_loudly():
@@ -50,3 +51,16 @@ def test_no_device_fails_loudly():
     assert e.value.code == 6
     with pytest.raises(S.SlcsError):
         S.steady_ant(np.array([1, 0], np.int32), np.array([0, 1], np.int32))
+    with pytest.raises(S.SlcsError) as e:
+        S.Server()
+    assert e.value.code == 6
+
+
+def test_struct_layouts_match_header():
+    """The ctypes mirrors have the sizes the C structs have (x86-64 ABI)."""
+    from semilocal_b200 import _lib
+    assert ctypes.sizeof(_lib.Query) == 12
+    assert ctypes.sizeof(_lib.Opts) == 32
+    assert ctypes.sizeof(_lib.ServerOpts) == 72
+    assert ctypes.sizeof(_lib.Result) == 64
+    assert ctypes.sizeof(_lib.ServerStats) == 96
