@@ -444,7 +444,94 @@ def run_suite(torch, S, peak_cells, peaks):
                           "bit_gcups": round(len(tbit_a) * len(tbit_b) / tb / 1e9, 2),
                           "bit_sample": "llcs_nary_symbol_smart_combing<uint64_t>, 2 bits/symbol, leading 2^17 x 2^17"}
     out["hybrid_pair_2p20"] = res
+    out["serving"] = run_serving(S, O, use_ref, ncpu)
     return out
+
+
+def _serving_query(r):
+    """Query of one generated request: kind uniform over global / string-substring / prefix-suffix, its
+    positions from the request's two uniform draws."""
+    m, n = len(r["a"]), len(r["b"])
+    if r["kind"] == "global":
+        return (0, 0, 0)
+    if r["kind"] == "string_substring":
+        i = int(r["u"] * n)
+        return (1, i, i + int(r["v"] * (n - i)))
+    return (2, int(r["u"] * m), int(r["v"] * n))
+
+
+def run_serving(S, O, use_ref, ncpu, count=160, rates=(20.0, None), server_opts=None):
+    """Poisson arrivals of comparison requests (|a| log-uniform [1k, 1M], 4 letters, b = a with 5 % subst +
+    1 % indels, query uniform over global / string-substring / prefix-suffix) through the serving loop.
+    Latency = result on the host minus the scheduled arrival.  rate None = every request at t = 0
+    (saturation throughput)."""
+    reqs = gen.serving_requests(count, 20.0, seed=6)
+    cells_all = sum(len(r["a"]) * len(r["b"]) for r in reqs)
+    base = np.array([r["t"] for r in reqs]) * 20.0   # unit-rate arrival times, rescaled per run
+    out = {"requests": count, "cells": cells_all, "lengths": "log-uniform [1e3, 1e6]"}
+    for rate in rates:
+        arrivals = base / rate if rate else np.zeros(count)
+        with S.Server(**(server_opts or {})) as srv:
+            t0 = srv.now()
+            tick_arrival, results, nxt = {}, {}, 0
+            while len(results) < count:
+                now = srv.now() - t0
+                while nxt < count and arrivals[nxt] <= now:
+                    r = reqs[nxt]
+                    t = srv.submit(r["a"], r["b"], _serving_query(r))
+                    tick_arrival[t] = (t0 + arrivals[nxt], nxt)
+                    nxt += 1
+                wait = 1 if nxt < count else 50
+                for res in srv.poll(timeout_ms=wait):
+                    results[res["ticket"]] = res
+            st = srv.stats()
+        lat = np.array([res["t_done"] - tick_arrival[t][0] for t, res in results.items()])
+        t_end = max(res["t_done"] for res in results.values())
+        bad = [res for res in results.values() if res["status"] != 0]
+        # answers of the smallest requests against the oracle's DP
+        small = sorted(results.items(), key=lambda kv: kv[1]["m"] * kv[1]["n"])[:6]
+        ok = all(res["score"] == _serving_dp(O, reqs[tick_arrival[t][1]]) for t, res in small)
+        out["poisson_%g_hz" % rate if rate else "saturation"] = {
+            "p50_ms": round(1e3 * float(np.percentile(lat, 50)), 2),
+            "p99_ms": round(1e3 * float(np.percentile(lat, 99)), 2),
+            "mean_ms": round(1e3 * float(lat.mean()), 2),
+            "gcups": round(cells_all / (t_end - t0) / 1e9, 1),
+            "wall_s": round(t_end - t0, 3), "failed": len(bad), "smallest_6_match_oracle": ok,
+            "launches": st["launches"], "peak_device_bytes": st["peak_bytes"], "budget_bytes": st["budget"]}
+    # the reference's own CPU combing on a bounded sample: the smallest requests, one after another, each with
+    # OpenMPIterativeCombing<int,false>(all host threads)
+    order = sorted(range(count), key=lambda i: len(reqs[i]["a"])) if ncpu > 0 else []
+    chosen, c = [], 0
+    for i in order:
+        cc = len(reqs[i]["a"]) * len(reqs[i]["b"])
+        if c + cc > 1.5e10:
+            break
+        chosen.append(i)
+        c += cc
+    t0 = time.perf_counter()
+    for i in chosen:
+        a, b = reqs[i]["a"].astype(np.int32), reqs[i]["b"].astype(np.int32)
+        if use_ref:
+            O.ref_comb(a, b, "openmp", ncpu)
+        else:
+            O.comb_antidiag(a, b, ncpu)
+    dt = time.perf_counter() - t0
+    if ncpu <= 0:
+        return out
+    out["cpu_ref"] = {"kind": "reference" if use_ref else "port", "threads": ncpu, "gcups": round(c / dt / 1e9, 2),
+                      "sample": f"the {len(chosen)} smallest requests ({c / 1e9:.1f} Gcells) in sequence, "
+                                f"OpenMPIterativeCombing<int,false>({ncpu})"}
+    return out
+
+
+def _serving_dp(O, r):
+    kind, i, j = _serving_query(r)
+    a, b = r["a"], r["b"]
+    if kind == 0:
+        return O.lcs_dp(a, b)
+    if kind == 1:
+        return O.lcs_dp(a, b[i:j])
+    return O.lcs_dp(a[:i], b[j:])
 
 
 # ------------------------------------------------------------------------------------------------------

@@ -194,8 +194,8 @@ int slcs_pair_plan_destroy(slcs_pair_plan *pl);
  * on its braid; the result is what SemiLocalStrategy::compute (R:include/SemiLocal/SemiLocalLCS.h:7-11)
  * followed by the score readout (R:include/LCS/LCS.h:223-233, R:approximate_matching/utils.h:281-334)
  * gives.  A worker thread admits requests by a device-memory budget, batches the small ones into
- * persistent combing launches on several streams (requests at or above big_cells cells run alone on their
- * own stream), overlaps the launches on the device, and keeps every finished braid resident for further
+ * persistent combing launches on several streams (requests at or above big_cells cells run alone on the
+ * big streams), overlaps the launches on the device, and keeps every finished braid resident for further
  * queries until it is released or evicted (least recently used first) to make room.  Results do not
  * depend on what else runs. */
 typedef struct slcs_server slcs_server;
@@ -205,10 +205,11 @@ typedef struct slcs_server_opts {
     int32_t small_streams;  /* concurrent batches of small requests (0: 2, at most 16) */
     int64_t big_cells;      /* m*n at or above which a request runs alone on the big stream (0: 2^32) */
     int32_t big_warps;      /* persistent-grid cap of a big launch, in warps (0: half the resident warps) */
-    int32_t small_warps;    /* persistent-grid cap of a small batch (0: half the resident warps) */
+    int32_t small_warps;    /* persistent-grid cap of a small batch (0: a quarter of the resident warps) */
     int32_t max_batch;      /* requests per small batch (0: 1024) */
     int32_t band_rows;      /* rows per band (0: chosen per request) */
-    int32_t reserved[8];
+    int32_t big_streams;    /* concurrent big requests (0: 2, at most 8) */
+    int32_t reserved[7];
 } slcs_server_opts;
 typedef struct slcs_result {
     uint64_t ticket;

@@ -41,7 +41,8 @@ class Query(ctypes.Structure):
 class ServerOpts(ctypes.Structure):
     _fields_ = [("mem_budget", ctypes.c_int64), ("max_pending", ctypes.c_int32), ("small_streams", ctypes.c_int32),
                 ("big_cells", ctypes.c_int64), ("big_warps", ctypes.c_int32), ("small_warps", ctypes.c_int32),
-                ("max_batch", ctypes.c_int32), ("band_rows", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8)]
+                ("max_batch", ctypes.c_int32), ("band_rows", ctypes.c_int32), ("big_streams", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 7)]
 
 
 class Result(ctypes.Structure):

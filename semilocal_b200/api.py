@@ -314,11 +314,12 @@ class Server:
     """
 
     def __init__(self, mem_budget: int = 0, small_streams: int = 0, big_cells: int = 0, max_batch: int = 0,
-                 big_warps: int = 0, small_warps: int = 0, band_rows: int = 0, max_pending: int = 0):
+                 big_warps: int = 0, small_warps: int = 0, band_rows: int = 0, max_pending: int = 0,
+                 big_streams: int = 0):
         self._h = ctypes.c_void_p()
         o = _lib.ServerOpts(mem_budget=mem_budget, max_pending=max_pending, small_streams=small_streams,
                             big_cells=big_cells, big_warps=big_warps, small_warps=small_warps, max_batch=max_batch,
-                            band_rows=band_rows)
+                            band_rows=band_rows, big_streams=big_streams)
         _lib.check(_lib.lib().slcs_server_create(ctypes.byref(o), ctypes.byref(self._h)))
         self._sizes = {}
 

@@ -5,10 +5,11 @@
 //   * admits them by a device-memory budget (inputs, strands and scratch while in flight, the braid while
 //     resident), evicting least recently used resident braids when the budget is short;
 //   * launches admitted requests as soon as a stream is free: requests of at least big_cells cells run alone
-//     on the big stream, the others are batched (largest first) into one persistent combing launch on one of
-//     the small streams.  Each launch caps its persistent grid, so a long big launch leaves SMs to the small
-//     batches and their work overlaps on the device; requests that arrive while launches run are admitted
-//     into the next launch of a stream that frees up;
+//     on one of the big streams (two by default), the others are batched (largest first) into one persistent
+//     combing launch on one of the small streams.  Each launch caps its persistent grid (big: half the
+//     resident warps, small: a quarter), so long big launches leave SMs to the small batches and their work
+//     overlaps on the device; requests that arrive while launches run are admitted into the next launch of a
+//     stream that frees up;
 //   * after each launch: c2r -> r2c, the request's query, 4 bytes back to the host per request;
 //   * keeps every finished braid resident (r2c, m+n int32) for further queries until it is released or
 //     evicted.
@@ -197,7 +198,8 @@ struct slcs_server {
     // worker-owned
     std::thread worker;
     std::deque<Req *> pending;
-    std::vector<cudaStream_t> streams;   // [0] big, [1..] small
+    int nbig = 1;
+    std::vector<cudaStream_t> streams;   // [0, nbig) big, [nbig, ..) small
     std::vector<Launch *> inflight;      // one launch per stream at most
     // resident braids and the budget
     std::mutex rmu;
@@ -417,20 +419,23 @@ bool schedule(slcs_server *S) {
     bool did = false;
     const int W = S->resident_warps;
     auto big = [&](const Req *r) { return r->cells >= S->o.big_cells; };
-    // the big stream: the oldest big request that fits
-    if (!S->inflight[0]) {
+    // big streams: the oldest big request that fits, one per free big stream
+    for (int idx = 0; idx < S->nbig; ++idx) {
+        if (S->inflight[idx]) continue;
+        bool launched = false;
         for (auto it = S->pending.begin(); it != S->pending.end(); ++it) {
             if (!big(*it)) continue;
-            if (!reserve(S, (*it)->need, S->streams[0])) break;
+            if (!reserve(S, (*it)->need, S->streams[idx])) break;
             std::vector<Req *> g{*it};
             S->pending.erase(it);
-            launch_group(S, 0, g, S->o.big_warps > 0 ? S->o.big_warps : W / 2);
-            did = true;
+            launch_group(S, idx, g, S->o.big_warps > 0 ? S->o.big_warps : W / 2);
+            did = launched = true;
             break;
         }
+        if (!launched) break;
     }
     // small streams: everything small that fits, oldest first, up to max_batch per launch
-    for (size_t idx = 1; idx < S->streams.size(); ++idx) {
+    for (size_t idx = S->nbig; idx < S->streams.size(); ++idx) {
         if (S->inflight[idx]) continue;
         std::vector<Req *> g;
         for (auto it = S->pending.begin(); it != S->pending.end() && (int) g.size() < S->o.max_batch;) {
@@ -443,7 +448,7 @@ bool schedule(slcs_server *S) {
             it = S->pending.erase(it);
         }
         if (g.empty()) break;
-        launch_group(S, (int) idx, g, S->o.small_warps > 0 ? S->o.small_warps : W / 2);
+        launch_group(S, (int) idx, g, S->o.small_warps > 0 ? S->o.small_warps : W / 4);
         did = true;
     }
     {
@@ -516,6 +521,7 @@ int slcs_server_create(const slcs_server_opts *opts, slcs_server **out) {
     if (S->o.small_streams > 16) S->o.small_streams = 16;
     if (S->o.big_cells <= 0) S->o.big_cells = (int64_t) 1 << 32;
     if (S->o.max_batch <= 0) S->o.max_batch = 1024;
+    S->nbig = S->o.big_streams > 0 ? std::min(S->o.big_streams, 8) : 2;
     S->device = E->device;
     S->t0 = std::chrono::steady_clock::now();
     S->resident_warps = comb_resident_warps(E);
@@ -525,7 +531,7 @@ int slcs_server_create(const slcs_server_opts *opts, slcs_server **out) {
         return fail(SLCS_ERR_CUDA, "cudaMemGetInfo failed");
     }
     S->budget = S->o.mem_budget > 0 ? S->o.mem_budget : (int64_t) (free_b / 2);
-    S->streams.assign(1 + S->o.small_streams, nullptr);
+    S->streams.assign(S->nbig + S->o.small_streams, nullptr);
     S->inflight.assign(S->streams.size(), nullptr);
     for (auto &s : S->streams)
         if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
