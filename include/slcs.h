@@ -243,6 +243,28 @@ double slcs_server_now(slcs_server *srv);
 /* Cancels requests not yet admitted, finishes those on the device, frees everything. */
 int slcs_server_destroy(slcs_server *srv);
 
+/* ---- autotuner (no counterpart in the reference) ------------------------------------------------- */
+/* Per device, the parameters an entry point uses when the caller passes 0: band heights by row-count class
+ * (for pairs that share a launch -- batches, hybrid tiles, serving -- and for one pair alone), the hybrid
+ * tile edge and the steady-ant shared-memory cutoff.  slcs_autotune() times the candidates on synthetic
+ * inputs (a few seconds) and installs the fastest; get/set let a caller persist and restore a table
+ * (set(NULL) restores the built-in defaults).  Zero entries mean "built-in default". */
+typedef struct slcs_tuning {
+    int32_t band_rows_batch[32];    /* rows per band (32 R) for a pair with ceil(log2 m) = k in a shared launch */
+    int32_t band_rows_single[32];   /* the same for one pair alone on the device (wavefront plans) */
+    int32_t tile;                   /* hybrid tile edge */
+    int32_t sa_cutoff;              /* steady-ant sub-problem size finished in shared memory (<= 4096) */
+    int32_t reserved[6];
+} slcs_tuning;
+#define SLCS_TUNE_BANDS_BATCH 1
+#define SLCS_TUNE_BANDS_SINGLE 2
+#define SLCS_TUNE_TILE 4
+#define SLCS_TUNE_SA_CUTOFF 8
+#define SLCS_TUNE_ALL 15
+int slcs_autotune(int flags, slcs_tuning *out);
+int slcs_tuning_get(slcs_tuning *out);
+int slcs_tuning_set(const slcs_tuning *in);
+
 /* ---- measurement helper (no counterpart in the reference) --------------------------------------- */
 /* Issue-rate ceiling of the combing cell's instruction mix on this device, in cells per second
  * (independent cells at full occupancy): the denominator of the combing kernels' roofline fraction. */

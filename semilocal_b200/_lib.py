@@ -57,6 +57,13 @@ class ServerStats(ctypes.Structure):
                                              "cells")] + [("pending", ctypes.c_int32), ("inflight", ctypes.c_int32)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("band_rows_batch", ctypes.c_int32 * 32), ("band_rows_single", ctypes.c_int32 * 32),
+                ("tile", ctypes.c_int32), ("sa_cutoff", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
+
+
+TUNE_BANDS_BATCH, TUNE_BANDS_SINGLE, TUNE_TILE, TUNE_SA_CUTOFF, TUNE_ALL = 1, 2, 4, 8, 15
+
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _i64p = ctypes.POINTER(ctypes.c_int64)
 _u8p = ctypes.POINTER(ctypes.c_uint8)
@@ -110,6 +117,9 @@ SIGNATURES = {
     "slcs_server_release": [_vp, ctypes.c_uint64],
     "slcs_server_stats_get": [_vp, ctypes.POINTER(ServerStats)],
     "slcs_server_destroy": [_vp],
+    "slcs_autotune": [_int, ctypes.POINTER(Tuning)],
+    "slcs_tuning_get": [ctypes.POINTER(Tuning)],
+    "slcs_tuning_set": [ctypes.POINTER(Tuning)],
 }
 # name -> (argtypes, restype) for entry points that do not return a status
 OTHER_SIGNATURES = {

@@ -394,3 +394,65 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def tuning() -> dict:
+    """The current device's tuning table (zeros = built-in defaults)."""
+    t = _lib.Tuning()
+    check(lib().slcs_tuning_get(ctypes.byref(t)))
+    return {"band_rows_batch": list(t.band_rows_batch), "band_rows_single": list(t.band_rows_single),
+            "tile": t.tile, "sa_cutoff": t.sa_cutoff}
+
+
+def set_tuning(table: Optional[dict]) -> None:
+    """Installs a tuning table (None restores the built-in defaults)."""
+    if table is None:
+        check(lib().slcs_tuning_set(None))
+        return
+    t = _lib.Tuning()
+    for i, v in enumerate(table.get("band_rows_batch", [])[:32]):
+        t.band_rows_batch[i] = int(v)
+    for i, v in enumerate(table.get("band_rows_single", [])[:32]):
+        t.band_rows_single[i] = int(v)
+    t.tile = int(table.get("tile", 0))
+    t.sa_cutoff = int(table.get("sa_cutoff", 0))
+    check(lib().slcs_tuning_set(ctypes.byref(t)))
+
+
+def autotune(flags: int = _lib.TUNE_ALL, cache: Optional[str] = None) -> dict:
+    """Measures and installs the tuning table of the current device.  With `cache` (a JSON file path) a table
+    saved for the same device name and library version is loaded instead of measuring, and a measured table
+    is saved there."""
+    import json
+    import os
+    key = None
+    if cache:
+        try:
+            import torch
+            key = f"{torch.cuda.get_device_name()}|v{lib().slcs_version()}"
+        except Exception:
+            key = f"device|v{lib().slcs_version()}"
+        if os.path.exists(cache):
+            try:
+                with open(cache) as f:
+                    saved = json.load(f)
+                if key in saved:
+                    set_tuning(saved[key])
+                    return saved[key]
+            except (OSError, ValueError):
+                pass
+    t = _lib.Tuning()
+    check(lib().slcs_autotune(flags, ctypes.byref(t)))
+    table = tuning()
+    if cache:
+        saved = {}
+        if os.path.exists(cache):
+            try:
+                with open(cache) as f:
+                    saved = json.load(f)
+            except (OSError, ValueError):
+                saved = {}
+        saved[key] = table
+        with open(cache, "w") as f:
+            json.dump(saved, f)
+    return table

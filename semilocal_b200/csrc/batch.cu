@@ -126,7 +126,8 @@ int slcs_batch_create(const int32_t *m, const int32_t *n, int npairs, int mode, 
         if (m[i] == 0 || n[i] == 0) bt->empty.push_back(i);
     }
     bt->total = bt->out_off[npairs];
-    const int Rmax = (opts && opts->band_rows) ? std::max(1, opts->band_rows / 32) : 32;
+    // length buckets: every pair gets the band height tuned for its row count (or the caller's)
+    const int Rforce = (opts && opts->band_rows) ? std::max(1, opts->band_rows / 32) : 0;
     std::vector<int> order(npairs);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(),
@@ -135,7 +136,7 @@ int slcs_batch_create(const int32_t *m, const int32_t *n, int npairs, int mode, 
     for (int oi = 0; oi < npairs; ++oi) {
         const int p = order[oi];
         if (m[p] > 0 && n[p] > 0) {
-            bt->prog_total += plan_bands(p, m[p], Rmax, bt->items);
+            bt->prog_total += plan_bands(p, m[p], Rforce ? Rforce : pick_rows_batch(m[p]), bt->items);
             if (mode == 1) bt->item_begin.push_back((int) bt->items.size());
         }
     }

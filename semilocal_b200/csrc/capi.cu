@@ -80,12 +80,6 @@ int check_dev_err(const int *d_err, cudaStream_t s) {
 
 namespace {
 
-int default_rows_per_lane(int rows) {
-    // enough bands to spread one pair over the device, but long bands for throughput
-    int R = 1;
-    while (R < 32 && 32 * 64 * R * 2 <= rows) R *= 2;
-    return R;
-}
 
 // Combing of one pair on device memory: d_r2c (m+n) receives row->col, d_c2r (optional) col->row,
 // d_score (optional, must be zeroed by the caller) the global LLCS.
@@ -94,8 +88,8 @@ int comb_wavefront_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int3
                        int32_t *d_score, const slcs_opts *opts, cudaStream_t s) {
     const int size = m + n;
     // orientation: rows = the string giving the shorter pipeline (64 steps per band + columns)
-    const int Ra = (opts && opts->band_rows) ? std::max(1, opts->band_rows / 32) : default_rows_per_lane(m);
-    const int Rb = (opts && opts->band_rows) ? std::max(1, opts->band_rows / 32) : default_rows_per_lane(n);
+    const int Ra = (opts && opts->band_rows) ? std::max(1, opts->band_rows / 32) : pick_rows_single(m);
+    const int Rb = (opts && opts->band_rows) ? std::max(1, opts->band_rows / 32) : pick_rows_single(n);
     const long long cost_ab = 64ll * ((m + 32 * Ra - 1) / (32 * Ra)) + n;
     const long long cost_ba = 64ll * ((n + 32 * Rb - 1) / (32 * Rb)) + m;
     const bool swap = cost_ba < cost_ab;
@@ -135,8 +129,8 @@ int comb_wavefront_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int3
 template <typename T>
 int comb_hybrid_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int32_t *d_r2c, int32_t *d_c2r,
                     int32_t *d_score, const slcs_opts *opts, cudaStream_t s) {
-    const int tr = (opts && opts->tile_rows > 0) ? opts->tile_rows : 4096;
-    const int tc = (opts && opts->tile_cols > 0) ? opts->tile_cols : 4096;
+    const int tr = (opts && opts->tile_rows > 0) ? opts->tile_rows : pick_tile();
+    const int tc = (opts && opts->tile_cols > 0) ? opts->tile_cols : pick_tile();
     HybridPlan *H = nullptr;
     SLCS_TRY(hybrid_plan_create(m, n, tr, tc, E, s, &H));
     DevBuf<int> err;

@@ -257,7 +257,7 @@ int hybrid_plan_create(int m, int n, int tile_rows, int tile_cols, Engine *E, cu
     int nprog = 0;
     for (size_t t = 0; t < cur.size(); ++t) {
         H->pairs_host[t] = CombPair{nullptr, nullptr, nullptr, nullptr, nullptr, cur[t].m, cur[t].n};
-        nprog += plan_bands((int) t, cur[t].m, 32, H->items);
+        nprog += plan_bands((int) t, cur[t].m, pick_rows_batch(cur[t].m), H->items);
     }
     H->nprog = nprog;
     H->resident = comb_resident_warps(E);

@@ -115,10 +115,7 @@ int slcs_pair_plan_create(int m, int n, int kind, const slcs_opts *opts, slcs_pa
     if ((rc = dalloc(reinterpret_cast<void **>(&P->d_err), sizeof(int), s))) return bail(rc);
     if (cudaMemsetAsync(P->d_err, 0, sizeof(int), s) != cudaSuccess) return bail(fail(SLCS_ERR_CUDA, "memset"));
     if (kind == SLCS_ALGO_WAVEFRONT) {
-        int R = 1;
-        if (opts && opts->band_rows > 0) R = std::max(1, opts->band_rows / 32);
-        else
-            while (R < 32 && 32 * 64 * R * 2 <= m) R *= 2;
+        const int R = (opts && opts->band_rows > 0) ? std::max(1, opts->band_rows / 32) : pick_rows_single(m);
         P->bands = plan_bands(0, m, R, P->items);
         P->resident = comb_resident_warps(E);
         if ((rc = dalloc(reinterpret_cast<void **>(&P->d_items), sizeof(CombItem) * P->items.size(), s)) ||
@@ -132,8 +129,8 @@ int slcs_pair_plan_create(int m, int n, int kind, const slcs_opts *opts, slcs_pa
             cudaEventCreate(&P->ev0) != cudaSuccess || cudaEventCreate(&P->ev1) != cudaSuccess)
             return bail(fail(SLCS_ERR_CUDA, "plan setup failed"));
     } else if (kind == SLCS_ALGO_HYBRID) {
-        const int tr = (opts && opts->tile_rows > 0) ? opts->tile_rows : 4096;
-        const int tc = (opts && opts->tile_cols > 0) ? opts->tile_cols : 4096;
+        const int tr = (opts && opts->tile_rows > 0) ? opts->tile_rows : pick_tile();
+        const int tc = (opts && opts->tile_cols > 0) ? opts->tile_cols : pick_tile();
         if ((rc = hybrid_plan_create(m, n, tr, tc, E, s, &P->hyb)) || (rc = hybrid_enable_timing(P->hyb)))
             return bail(rc);
     } else {

@@ -498,12 +498,6 @@ void worker_main(slcs_server *S) {
     }
 }
 
-int default_rows_for(int m) {
-    // long bands: every band combs all n columns, so fewer, taller bands waste less pipeline fill
-    int R = 1;
-    while (R < 32 && 32 * 2 * R <= m) R *= 2;
-    return R;
-}
 
 }  // namespace
 
@@ -562,7 +556,7 @@ int slcs_server_submit(slcs_server *S, const uint8_t *a, int m, const uint8_t *b
     r->n = n;
     r->q = qq;
     r->cells = (int64_t) m * n;
-    r->R = S->o.band_rows > 0 ? std::max(1, std::min(32, S->o.band_rows / 32)) : default_rows_for(m);
+    r->R = S->o.band_rows > 0 ? std::max(1, std::min(32, S->o.band_rows / 32)) : pick_rows_batch(m);
     r->nbands = (m > 0 && n > 0) ? (m + 32 * r->R - 1) / (32 * r->R) + 1 : 0;
     r->need = req_need(m, n, r->nbands);
     r->keep = (int64_t) align_up(sizeof(int32_t) * (size_t) std::max(m + n, 1), 256);

@@ -110,6 +110,14 @@ struct DevBuf {
 };
 
 // ------------------------------------------------------------------------------------------------
+// tuning table of the current device (tune.cu): what a caller that passes 0 for a parameter gets
+// ------------------------------------------------------------------------------------------------
+int pick_rows_batch(int rows);    // rows per lane (band height / 32) for a pair sharing a launch
+int pick_rows_single(int rows);   // the same for one pair alone on the device
+int pick_tile();                  // hybrid tile edge
+int pick_sa_cutoff();             // steady-ant size finished in shared memory
+
+// ------------------------------------------------------------------------------------------------
 // combing (comb.cu)
 // ------------------------------------------------------------------------------------------------
 struct CombPair {
@@ -149,7 +157,7 @@ int launch_invert(const int32_t *c2r, int size, int32_t *r2c, bool rot180, int *
 // Batched unit-Monge products on device memory: problem i occupies [off[i], off[i] + n[i]) of the
 // concatenated row->col arrays d_P, d_Q and d_R (out).
 int steady_ant_batch_dev(const int32_t *d_P, const int32_t *d_Q, const std::vector<int64_t> &off,
-                         const std::vector<int> &n, int32_t *d_R, int *d_err, cudaStream_t s);
+                         const std::vector<int> &n, int32_t *d_R, int *d_err, cudaStream_t s, int cutoff = 0);
 int steady_ant_max_small();
 // Reusable plans: create() plans and allocates, run() only launches kernels on s (capturable).
 struct SaPlan;
@@ -160,7 +168,7 @@ struct SaScratch {
     int64_t elems = 0, tab = 0, vec = 0, cst = 0;
 };
 int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, SaPlan **out, cudaStream_t s,
-                   const SaScratch *shared);
+                   const SaScratch *shared, int cutoff = 0);   // cutoff 0: the tuned / default cutoff
 // shared != nullptr: the plan uses the caller's scratch; shared->elems < 0 defers the binding to sa_plan_bind.
 int sa_plan_bind(SaPlan *P, const SaScratch *shared);
 // Scratch sizes a plan needs (for building a shared SaScratch).

@@ -984,7 +984,14 @@ void sa_plan_destroy(SaPlan *P) {
 // Plans the batched unit-Monge products of problems i = 0..np-1, problem i occupying [off[i], off[i] + n[i])
 // of concatenated row->col arrays.  All task lists and scratch are built and allocated here.
 int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, SaPlan **out, cudaStream_t s,
-                   const SaScratch *shared) {
+                   const SaScratch *shared, int cutoff) {
+    // sub-problems of at most `cut` common indices finish in shared memory (a power of two <= kSaSB)
+    int cut = cutoff > 0 ? cutoff : pick_sa_cutoff();
+    {
+        int c = 256;
+        while (c * 2 <= cut && c < kSaSB) c <<= 1;
+        cut = c;
+    }
     *out = nullptr;
     auto P = new SaPlan();
     P->alloc_stream = s;
@@ -1003,10 +1010,10 @@ int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, S
     std::vector<SaTile> probtiles;
     std::vector<SaBlockItem> items;
     for (int i = 0; i < P->np; ++i) {
-        if (n[i] > 0 && n[i] <= kSaSB) P->small.push_back(i);
+        if (n[i] > 0 && n[i] <= cut) P->small.push_back(i);
         probs[i] = SaNode{off[i], n[i], n[i], 0, 0, 0, 0, 0};
         for (int t = 0; (int64_t) t * kMT < n[i]; ++t) probtiles.push_back(SaTile{i, t});
-        for (int b0 = 0; b0 < n[i]; b0 += kSaSB) items.push_back(SaBlockItem{off[i] + b0, std::min(kSaSB, n[i] - b0), 0});
+        for (int b0 = 0; b0 < n[i]; b0 += cut) items.push_back(SaBlockItem{off[i] + b0, std::min(cut, n[i] - b0), 0});
     }
     P->nprobtiles = (int) probtiles.size();
     P->nitems = (int) items.size();
@@ -1014,7 +1021,7 @@ int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, S
     std::vector<SaTile> tiles;
     std::vector<int2> tasks;
     std::vector<int64_t> copies;
-    for (int64_t size = kSaSB; size < P->maxn; size <<= 1) {
+    for (int64_t size = cut; size < P->maxn; size <<= 1) {
         const int64_t span = size << 1;
         SaLevel L{};
         L.size = size;
@@ -1206,9 +1213,9 @@ void sa_plan_needs(const SaPlan *P, int64_t *elems, int64_t *tab, int64_t *vec, 
 }
 
 int steady_ant_batch_dev(const int32_t *d_P, const int32_t *d_Q, const std::vector<int64_t> &off,
-                         const std::vector<int> &n, int32_t *d_R, int *d_err, cudaStream_t s) {
+                         const std::vector<int> &n, int32_t *d_R, int *d_err, cudaStream_t s, int cutoff) {
     SaPlan *P = nullptr;
-    SLCS_TRY(sa_plan_create(off, n, &P, s, nullptr));
+    SLCS_TRY(sa_plan_create(off, n, &P, s, nullptr, cutoff));
     int rc = sa_plan_run(P, d_P, d_Q, d_R, d_err, s);
     sa_plan_destroy(P);
     return rc;
@@ -1224,7 +1231,6 @@ extern "C" {
 
 int slcs_steady_ant_dev(const int32_t *d_p, const int32_t *d_q, int n, int32_t *d_r, const slcs_opts *opts,
                         void *stream) {
-    (void) opts;
     if (n < 0) return fail(SLCS_ERR_ARG, "negative size");
     if (n > 0 && (!d_p || !d_q || !d_r)) return fail(SLCS_ERR_ARG, "NULL buffer");
     if (n >= (1 << 30)) return fail(SLCS_ERR_TOO_LARGE, "n must be below 2^30");
@@ -1235,7 +1241,8 @@ int slcs_steady_ant_dev(const int32_t *d_p, const int32_t *d_q, int n, int32_t *
     DevBuf<int> err;
     SLCS_TRY(err.alloc(1, s));
     SLCS_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(int), s));
-    SLCS_TRY(steady_ant_batch_dev(d_p, d_q, std::vector<int64_t>{0}, std::vector<int>{n}, d_r, err.p, s));
+    SLCS_TRY(steady_ant_batch_dev(d_p, d_q, std::vector<int64_t>{0}, std::vector<int>{n}, d_r, err.p, s,
+                                  opts ? opts->sa_cutoff : 0));
     return check_dev_err(err.p, s);
 }
 

@@ -64,3 +64,4 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(_lib.ServerOpts) == 72
     assert ctypes.sizeof(_lib.Result) == 64
     assert ctypes.sizeof(_lib.ServerStats) == 96
+    assert ctypes.sizeof(_lib.Tuning) == 288
