@@ -27,6 +27,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from semilocal_b200 import gen  # noqa: E402
+from semilocal_b200.shard import max_over_ranks  # noqa: E402
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 OPS_PER_CELL = 5     # compare, compare, or, two selects (R:include/SemiLocal/SemiLocalLCS.h:158-172)
@@ -179,6 +180,10 @@ def run_ours(args, rank, world, local):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
 
+    # band heights by length class, hybrid tile and steady-ant cutoff for this device (outside timing)
+    t_tune = time.perf_counter()
+    table = S.autotune(cache=args.tuning_cache or None)
+    t_tune = time.perf_counter() - t_tune
     pairs = batch_workload(5 + 1000 * rank)
     a_cat, a_off, ms, b_cat, b_off, ns = S.concat_pairs(pairs)
     # pinned host copies for the end-to-end leg
@@ -220,11 +225,7 @@ def run_ours(args, rank, world, local):
     # correctness spot check of the timed plan against the oracle on a few pairs
     plan.download(out_pin.numpy(), sc_pin.numpy(), sh)
     torch.cuda.synchronize()
-    t_max = total_ms
-    if dist is not None:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max = max_over_ranks(total_ms, dist, "cuda")
     ms_per_step = t_max / args.steps
     value = cells * world / (ms_per_step * 1e-3) / 1e9
 
@@ -244,11 +245,7 @@ def run_ours(args, rank, world, local):
             plan.download(out_pin.numpy(), sc_pin.numpy(), sh)
         e1.record(stream)
     e1.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, dist, "cuda")
     e2e_value = cells * world / (e2e_ms * 1e-3) / 1e9
 
     # ---- plain per-pair launches on the same plan (baseline for the batched launch) ----
@@ -283,7 +280,10 @@ def run_ours(args, rank, world, local):
                                "b = a with 10% subst + 1% indels; int32 braids; persistent length-bucketed "
                                "launch replayed from a CUDA graph",
                    "pairs_per_gpu": len(pairs), "cells_per_gpu": cells, "parallelism": f"pairs sharded, {world} GPU",
-                   "l2": "inputs + braids (~%d MB) exceed the 126 MB L2" % ((a_cat.nbytes + b_cat.nbytes + 8 * plan.total) >> 20)},
+                   "l2": "inputs + braids (~%d MB) exceed the 126 MB L2" % ((a_cat.nbytes + b_cat.nbytes + 8 * plan.total) >> 20),
+                   "tuning": {"band_rows_by_log2_len": {str(k): table["band_rows_batch"][k] for k in range(8, 17)},
+                              "hybrid_tile": table["tile"], "steady_ant_cutoff": table["sa_cutoff"],
+                              "autotune_s": round(t_tune, 2)}},
         "e2e": {"value": round(e2e_value, 2), "unit": "GCUPS", "h2d_bytes_per_step": info["h2d_bytes"],
                 "d2h_bytes_per_step": info["d2h_bytes"]},
         "gpu_launches": info["launches"] * args.steps,
@@ -575,6 +575,8 @@ def main():
     ap.add_argument("--ref-step-s", type=float, default=6.0, help="seconds of CPU work per reference step")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-suite", action="store_true", help="skip the plain / steady-ant / hybrid workloads")
+    ap.add_argument("--tuning-cache", default="", help="JSON file: load the autotuned table if saved there for "
+                                                        "this device, else measure and save it")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -78,7 +78,55 @@ struct Timer {
     }
 };
 
-// ms of one batched run of np pairs of L x L cells at band height 32 R (the second of two runs)
+// the fastest of three timed runs of fn (CUDA events on s)
+template <typename F>
+int best_of(cudaStream_t s, float *ms, F fn) {
+    Timer T;
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+        float t = 0;
+        if (cudaEventRecord(T.e0, s) != cudaSuccess) return fail(SLCS_ERR_CUDA, "tuning timing failed");
+        SLCS_TRY(fn());
+        if (cudaEventRecord(T.e1, s) != cudaSuccess || cudaEventSynchronize(T.e1) != cudaSuccess ||
+            cudaEventElapsedTime(&t, T.e0, T.e1) != cudaSuccess)
+            return fail(SLCS_ERR_CUDA, "tuning timing failed");
+        best = std::min(best, t);
+    }
+    *ms = best;
+    return SLCS_OK;
+}
+
+// The candidate to install: the fastest, unless the built-in default is within 3 % of it (timing noise must
+// not move a parameter away from its default).
+int choose(const std::vector<std::pair<int, float>> &timed, int dflt) {
+    float best = 1e30f, tdef = -1;
+    int arg = dflt;
+    for (const auto &c : timed) {
+        if (c.second < best) {
+            best = c.second;
+            arg = c.first;
+        }
+        if (c.first == dflt) tdef = c.second;
+    }
+    return (tdef >= 0 && tdef <= 1.03f * best) ? dflt : arg;
+}
+
+// Warps of the combing kernel resident on the current device at once (cached per device).
+int resident_warps_now() {
+    static int cache[64] = {0};
+    const int d = cur_device();
+    if (!cache[d]) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d) != cudaSuccess || sms <= 0) {
+            cudaGetLastError();
+            return 1 << 30;
+        }
+        cache[d] = comb_resident_warps_sm(sms);
+    }
+    return cache[d];
+}
+
+// ms of one batched run of np pairs of L x L cells at band height 32 R (the fastest of three)
 int time_batch(int L, int np, int R, cudaStream_t s, float *ms) {
     std::vector<int32_t> m(np, L), n(np, L);
     std::vector<int64_t> off(np);
@@ -97,19 +145,13 @@ int time_batch(int L, int np, int R, cudaStream_t s, float *ms) {
     slcs_batch *bt = nullptr;
     SLCS_TRY(slcs_batch_create(m.data(), n.data(), np, 0, &o, &bt));
     int rc = slcs_batch_upload(bt, acat.data(), off.data(), bcat.data(), off.data(), s);
-    Timer T;
-    for (int rep = 0; rep < 2 && rc == SLCS_OK; ++rep) {
-        cudaEventRecord(T.e0, s);
-        rc = slcs_batch_run(bt, 0, s);
-        cudaEventRecord(T.e1, s);
-    }
-    if (rc == SLCS_OK && (cudaEventSynchronize(T.e1) != cudaSuccess || cudaEventElapsedTime(ms, T.e0, T.e1) != cudaSuccess))
-        rc = fail(SLCS_ERR_CUDA, "tuning timing failed");
+    if (rc == SLCS_OK) rc = slcs_batch_run(bt, 0, s);   // warm-up
+    if (rc == SLCS_OK) rc = best_of(s, ms, [&] { return slcs_batch_run(bt, 0, s); });
     slcs_batch_destroy(bt);
     return rc;
 }
 
-// ms of one single-pair plan run (kind, opts) on an L x L pair (the second of two runs)
+// ms of one single-pair plan run (kind, opts) on an L x L pair (the fastest of three)
 int time_pair(int L, int kind, const slcs_opts &o, cudaStream_t s, float *ms) {
     std::vector<uint8_t> a, b;
     random_symbols(a, L, 77);
@@ -126,15 +168,9 @@ int time_pair(int L, int kind, const slcs_opts &o, cudaStream_t s, float *ms) {
         if (cudaMemcpyAsync(da, a.data(), L, cudaMemcpyHostToDevice, s) != cudaSuccess ||
             cudaMemcpyAsync(db, b.data(), L, cudaMemcpyHostToDevice, s) != cudaSuccess)
             rc = fail(SLCS_ERR_CUDA, "tuning upload failed");
-        Timer T;
-        for (int rep = 0; rep < 2 && rc == SLCS_OK; ++rep) {
-            cudaEventRecord(T.e0, s);
-            rc = slcs_pair_plan_run(pl, da, db, dr, dsc, 0, s);
-            cudaEventRecord(T.e1, s);
-        }
+        if (rc == SLCS_OK) rc = slcs_pair_plan_run(pl, da, db, dr, dsc, 0, s);   // warm-up
+        if (rc == SLCS_OK) rc = best_of(s, ms, [&] { return slcs_pair_plan_run(pl, da, db, dr, dsc, 0, s); });
         if (rc == SLCS_OK) rc = slcs_pair_plan_check(pl, s);
-        if (rc == SLCS_OK && cudaEventElapsedTime(ms, T.e0, T.e1) != cudaSuccess)
-            rc = fail(SLCS_ERR_CUDA, "tuning timing failed");
     }
     dfree(da, s);
     dfree(db, s);
@@ -166,15 +202,9 @@ int time_sa(int n, int cutoff, cudaStream_t s, float *ms) {
             cudaMemcpyAsync(dq, q.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
             cudaMemsetAsync(derr, 0, sizeof(int), s) != cudaSuccess)
             rc = fail(SLCS_ERR_CUDA, "tuning upload failed");
-        Timer T;
-        for (int rep = 0; rep < 2 && rc == SLCS_OK; ++rep) {
-            cudaEventRecord(T.e0, s);
-            rc = sa_plan_run(P, dp, dq, dr, derr, s);
-            cudaEventRecord(T.e1, s);
-        }
+        if (rc == SLCS_OK) rc = sa_plan_run(P, dp, dq, dr, derr, s);   // warm-up
+        if (rc == SLCS_OK) rc = best_of(s, ms, [&] { return sa_plan_run(P, dp, dq, dr, derr, s); });
         if (rc == SLCS_OK) rc = check_dev_err(derr, s);
-        if (rc == SLCS_OK && cudaEventElapsedTime(ms, T.e0, T.e1) != cudaSuccess)
-            rc = fail(SLCS_ERR_CUDA, "tuning timing failed");
     }
     if (P) sa_plan_destroy(P);
     dfree(dp, s);
@@ -193,9 +223,17 @@ int pick_rows_batch(int rows) {
 }
 
 int pick_rows_single(int rows) {
-    std::lock_guard<std::mutex> lk(g_tmu);
-    const int v = g_tab[cur_device()].band_rows_single[log2_class(std::max(rows, 1))];
-    return v > 0 ? std::max(1, std::min(32, v / 32)) : default_rows_single(rows);
+    int R;
+    {
+        std::lock_guard<std::mutex> lk(g_tmu);
+        const int v = g_tab[cur_device()].band_rows_single[log2_class(std::max(rows, 1))];
+        R = v > 0 ? std::max(1, std::min(32, v / 32)) : default_rows_single(rows);
+    }
+    // a lone pair's bands must all be resident at once: a band beyond the resident warps starts only when
+    // a warp finishes a whole band, which doubles the time
+    const int64_t W = resident_warps_now();
+    while (R < 32 && ((int64_t) rows + 32 * R - 1) / (32 * R) > W) R *= 2;
+    return R;
 }
 
 int pick_tile() {
@@ -248,80 +286,70 @@ int slcs_autotune(int flags, slcs_tuning *out) {
         std::lock_guard<std::mutex> lk(g_tmu);
         T = g_tab[E->device];
     }
-    // 1. band height for pairs sharing a launch: L x L pairs, about 2^31 cells per launch (at most 4096 pairs)
+    const int W = comb_resident_warps(E);
+    // 1. band height for pairs sharing a launch, classes 2^8 .. 2^14: L x L pairs, enough of them for at least
+    //    four waves of bands (a tuned height must hold in a launch much larger than the device); longer pairs
+    //    keep the default (32 rows per lane)
     if (flags & SLCS_TUNE_BANDS_BATCH) {
-        for (int k = 8; k <= 16; ++k) {
+        for (int k = 8; k <= 14; ++k) {
             const int L = 1 << k;
-            const int np = (int) std::max<int64_t>(1, std::min<int64_t>(4096, (1ll << 31) / ((int64_t) L * L)));
-            float best = 1e30f;
-            int bestR = 32;
+            const int bands32 = (L + 1023) / 1024;
+            const int np = (int) std::min<int64_t>(32768, std::max<int64_t>((4ll * W + bands32 - 1) / bands32,
+                                                                            (1ll << 31) / ((int64_t) L * L)));
+            std::vector<std::pair<int, float>> timed;
             for (int R = 1; R <= 32; R *= 2) {
-                if (32 * R > 2 * L) break;
+                if (32 * R > 2 * L || (L >= 4096 && R < 4)) continue;
                 float ms = 0;
                 SLCS_TRY(time_batch(L, np, R, s, &ms));
-                if (ms < best) {
-                    best = ms;
-                    bestR = R;
-                }
+                timed.emplace_back(R, ms);
             }
-            T.band_rows_batch[k] = 32 * bestR;
+            T.band_rows_batch[k] = 32 * choose(timed, 32);
         }
         for (int k = 0; k < 8; ++k) T.band_rows_batch[k] = T.band_rows_batch[8];
-        for (int k = 17; k < 32; ++k) T.band_rows_batch[k] = T.band_rows_batch[16];
+        for (int k = 15; k < 32; ++k) T.band_rows_batch[k] = 32 * 32;
     }
-    // 2. band height for one pair alone: L x L, classes 2^10 .. 2^18; above, the same number of bands
+    // 2. band height for one pair alone: L x L, classes 2^10 .. 2^19; each longer class doubles the height
+    //    (the same number of bands), and pick_rows_single keeps every band resident
     if (flags & SLCS_TUNE_BANDS_SINGLE) {
-        for (int k = 10; k <= 18; ++k) {
+        for (int k = 10; k <= 19; ++k) {
             const int L = 1 << k;
-            float best = 1e30f;
-            int bestR = 1;
+            std::vector<std::pair<int, float>> timed;
             for (int R = 1; R <= 32; R *= 2) {
-                if (32 * R > L) break;
+                if (32 * R > L || (k == 19 && R < 8)) continue;
                 slcs_opts o{};
                 o.algo = SLCS_ALGO_WAVEFRONT;
                 o.band_rows = 32 * R;
                 float ms = 0;
                 SLCS_TRY(time_pair(L, SLCS_ALGO_WAVEFRONT, o, s, &ms));
-                if (ms < best) {
-                    best = ms;
-                    bestR = R;
-                }
+                timed.emplace_back(R, ms);
             }
-            T.band_rows_single[k] = 32 * bestR;
+            T.band_rows_single[k] = 32 * choose(timed, default_rows_single(L));
         }
         for (int k = 0; k < 10; ++k) T.band_rows_single[k] = T.band_rows_single[10];
-        for (int k = 19; k < 32; ++k) T.band_rows_single[k] = std::min(1024, T.band_rows_single[k - 1] * 2);
+        for (int k = 20; k < 32; ++k) T.band_rows_single[k] = std::min(1024, T.band_rows_single[k - 1] * 2);
     }
     // 3. hybrid tile edge on a 2^17 x 2^17 pair
     if (flags & SLCS_TUNE_TILE) {
-        float best = 1e30f;
-        int bestT = 4096;
+        std::vector<std::pair<int, float>> timed;
         for (int tile : {2048, 4096, 8192}) {
             slcs_opts o{};
             o.algo = SLCS_ALGO_HYBRID;
             o.tile_rows = o.tile_cols = tile;
             float ms = 0;
             SLCS_TRY(time_pair(1 << 17, SLCS_ALGO_HYBRID, o, s, &ms));
-            if (ms < best) {
-                best = ms;
-                bestT = tile;
-            }
+            timed.emplace_back(tile, ms);
         }
-        T.tile = bestT;
+        T.tile = choose(timed, 4096);
     }
     // 4. steady-ant cutoff on two random 2^20 permutations
     if (flags & SLCS_TUNE_SA_CUTOFF) {
-        float best = 1e30f;
-        int bestC = steady_ant_max_small();
+        std::vector<std::pair<int, float>> timed;
         for (int c = 1024; c <= steady_ant_max_small(); c *= 2) {
             float ms = 0;
             SLCS_TRY(time_sa(1 << 20, c, s, &ms));
-            if (ms < best) {
-                best = ms;
-                bestC = c;
-            }
+            timed.emplace_back(c, ms);
         }
-        T.sa_cutoff = bestC;
+        T.sa_cutoff = choose(timed, steady_ant_max_small());
     }
     {
         std::lock_guard<std::mutex> lk(g_tmu);
