@@ -22,3 +22,11 @@ mkdir -p "$here/_ref"
   -I"$src" "$here/ref_shim.cpp" -o "$here/_ref/libslcs_ref.so.tmp" -Wl,--no-undefined
 mv "$here/_ref/libslcs_ref.so.tmp" "$here/_ref/libslcs_ref.so"
 echo "build_ref: wrote $here/_ref/libslcs_ref.so"
+# The reference's own strategies with the GPU engine plugged in through include/slcs.hpp (needs the engine).
+repo="$(cd "$here/.." && pwd)"
+if [ -f "$repo/semilocal_b200/libslcs.so" ]; then
+  /usr/bin/g++ -std=c++17 -O2 -march=x86-64-v3 -fopenmp -w -I"$src" -I"$repo/include" \
+    "$repo/tests/cpp/reference_plugin.cpp" -L"$repo/semilocal_b200" -lslcs \
+    -Wl,-rpath,'$ORIGIN/../../semilocal_b200' -o "$here/_ref/reference_plugin"
+  echo "build_ref: wrote $here/_ref/reference_plugin"
+fi
