@@ -31,6 +31,10 @@ from semilocal_b200.shard import max_over_ranks  # noqa: E402
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 OPS_PER_CELL = 5     # compare, compare, or, two selects (R:include/SemiLocal/SemiLocalLCS.h:158-172)
+# DRAM bytes (read + write) per cell of comb_kernel, from one ncu capture of the 256-pair batch case
+# (`python -m semilocal_b200.profile_cases batch 256`: 3.29 MB for 8.12e9 cells); a launch's traffic grows with
+# its bands x columns, i.e. with its cells at a fixed band height, so the bench scales it by cells.
+COMB_DRAM_BYTES_PER_CELL = 3.29e6 / 8.1177e9
 
 
 def dist_env():
@@ -290,7 +294,10 @@ def run_ours(args, rank, world, local):
         "plain_per_pair": {"value": round(plain_gcups, 2), "unit": "GCUPS", "launches": plain_info["launches"],
                            "batched_over_plain": round(value / world / plain_gcups, 2)},
         "roofline": {"bound": "int32-issue", "achieved": round(achieved_gops, 1), "peak": round(peak_gops, 1),
-                     "unit": "Gop/s", "frac": round(achieved_gops / peak_gops, 4), "traffic": None,
+                     "unit": "Gop/s", "frac": round(achieved_gops / peak_gops, 4),
+                     "traffic": int(COMB_DRAM_BYTES_PER_CELL * cells),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of comb_kernel on the "
+                                       "256-pair batch case, scaled to this launch by cells",
                      "kernel": "comb_kernel", "kernel_ms": round(k_ms, 3),
                      "peak_source": "slcs_probe_cell_peak (cell instruction mix, full occupancy), x5 ops/cell"},
         "clocks": clk.summary(),
