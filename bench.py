@@ -431,7 +431,9 @@ def run_suite(torch, S, peak_cells, peaks):
         ent = {"gpu_ms": round(ms, 2), "gcups": round(m * n / ms / 1e6, 1), "score": int(sc2.item()),
                "comb_kernel_ms": round(kms, 2), "launches": pl.launches()}
         if kind != S.PLAN_BITPARALLEL:
-            ent["int_frac_of_probe"] = round(m * n / (kms * 1e-3) / peak_cells, 4)
+            # whole run (tiles + glue for the hybrid) and combing kernel alone, against the cell-mix probe
+            ent["roofline_frac_whole_run"] = round(m * n / (ms * 1e-3) / peak_cells, 4)
+            ent["roofline_frac_comb_kernel"] = round(m * n / (kms * 1e-3) / peak_cells, 4)
             braids[name] = r2.cpu().numpy()
         res[name] = ent
         pl.close()

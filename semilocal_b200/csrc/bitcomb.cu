@@ -200,9 +200,10 @@ int strips_per_lane(int nstrips) {
         const int v = atoi(env);
         if (v == 1 || v == 2 || v == 4) return v;
     }
-    // more strips per lane = fewer bands and more independent work per warp; one pair has only
-    // ~n / (32 * skew) strips in flight, so small values keep more warps busy
-    if (nstrips >= 4 * 32 * 1024) return 2;
+    // more strips per lane = fewer bands and more independent work per warp, but a longer fill; one pair has
+    // only ~n / (32 * skew) strips in flight, so small pairs keep one strip per lane (measured on B200: a
+    // 2^20-row pair runs 7% faster with two, a 2^18-row pair is faster with one)
+    if (nstrips >= 32 * 1024) return 2;
     return 1;
 }
 

@@ -596,6 +596,34 @@ __global__ void __launch_bounds__(256) sa_scan_kernel(const SaNode *__restrict__
     }
 }
 
+// Exclusive prefix sums along g of 32 table columns per block (lanes = columns, so every row access is one
+// coalesced segment); the 8 warps take 8 consecutive row ranges and combine their column totals.
+__global__ void __launch_bounds__(256) sa_scan_cols_kernel(const SaNode *__restrict__ nodes,
+                                                           const int2 *__restrict__ groups, int32_t *__restrict__ tab) {
+    const int2 gr = groups[blockIdx.x];   // (node, first column)
+    const SaNode nd = nodes[gr.x];
+    const int W = nd.G + 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int h = gr.y + lane;
+    const bool act = h < W;
+    int32_t *col = tab + nd.tab_off + h;   // entry (g, h) at col[g W]
+    const int per = (W + 7) / 8, g0 = min(W, warp * per), g1 = min(W, g0 + per);
+    __shared__ int32_t part[8][32];
+    int sum = 0;
+    if (act)
+        for (int g = g0; g < g1; ++g) sum += col[(int64_t) g * W];
+    part[warp][lane] = sum;
+    __syncthreads();
+    int run = 0;
+    for (int w = 0; w < warp; ++w) run += part[w][lane];
+    if (act)
+        for (int g = g0; g < g1; ++g) {
+            const int v = col[(int64_t) g * W];
+            col[(int64_t) g * W] = run;
+            run += v;
+        }
+}
+
 __device__ __forceinline__ int hbm_delta_corner(const SaNode &nd, const int32_t *tab, const int32_t *vec, int g, int h) {
     // delta(g Sc, h Sc) = #{hi: row < g Sc, col < h Sc} - #{lo: row < g Sc, col < h Sc}
     //                    + #{lo: row < g Sc} + #{lo: col < h Sc} - #lo       (tab holds the signed prefix)
@@ -692,6 +720,7 @@ struct BandShared {
     int32_t y[kBandYCap];              // columns [clo, clo + ny): row | hi bit (when they fit)
     int32_t cst[kBandThreads + 1];     // c* at band rows kBandWalk * j; entry nwalk: the band's bottom
     int32_t queue[kBandThreads];       // walks left to whole warps
+    int32_t subcnt[kBandThreads / 32]; // rows of each sub-band raising delta at the band's bottom c*
     int nq;
 };
 
@@ -827,12 +856,20 @@ __global__ void __launch_bounds__(kBandThreads) sa_band_kernel(const SaNode *__r
     }
     __syncthreads();
     const YView Y{S.y, ys + nd.off, clo, ysm};
-    // c* at the sub-band tops (warp w >= 1: row R0 + w kBandSub)
+    // c* at the sub-band tops (warp w >= 1: row R0 + w kBandSub).  The rows between a top and the band's bottom
+    // that raise delta at cbot are counted once per sub-band (each warp its own), and summed over the warps below.
+    if (cbot <= k && warp * kBandSub < nr) {
+        const int i0 = warp * kBandSub, i1 = min(i0 + kBandSub, nr);
+        const int cnt = band_row_count(S.x, i0, i1, cbot, lane);
+        if (lane == 0) S.subcnt[warp] = cnt;
+    }
+    __syncthreads();
     if (warp >= 1 && warp * kBandSub < nr) {
         const int i = warp * kBandSub;
         int c = k + 1;
         if (cbot <= k) {
-            const int need = band_row_count(S.x, i, nr, cbot, lane);
+            int need = 0;
+            for (int w = warp; w < nwarps && w * kBandSub < nr; ++w) need += S.subcnt[w];
             c = band_col_search(Y, k, cbot, cend, need, R0 + i, lane);
         }
         if (lane == 0) S.cst[warp * wsub] = c;
@@ -1041,6 +1078,7 @@ int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, S
                 }
                 int Sc = 256;
                 while ((int64_t) Sc * Sc < k) Sc <<= 1;
+                while (Sc < kBand && k / Sc > 1024) Sc <<= 1;   // a (G+1)^2 table of at most ~1024^2 entries
                 const int G = (k + Sc - 1) / Sc;
                 nodes.push_back(SaNode{off[i] + a, k, h, Sc, G, L.tab_tot, L.vec_tot, L.cst_tot});
                 L.tab_tot += (int64_t) (G + 1) * (G + 1);
@@ -1060,7 +1098,7 @@ int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, S
         L.nl0 = (int) (tasks.size() - L.o_l0);
         L.o_l1 = (int64_t) tasks.size();
         for (int j = 0; j < L.nnodes; ++j)
-            for (int y = 0; y < nodes[first_node + j].G + 1; ++y) tasks.push_back(make_int2(j, y));
+            for (int y = 0; y < nodes[first_node + j].G + 1; y += 32) tasks.push_back(make_int2(j, y));
         L.nl1 = (int) (tasks.size() - L.o_l1);
         // band boundaries: from the table where they are multiples of Sc, else from the one below
         L.o_ct = (int64_t) tasks.size();
@@ -1171,7 +1209,7 @@ int sa_plan_run_ex(SaPlan *P, const int32_t *d_P, const int32_t *d_leafP, const 
             sa_map_kernel<<<L.ntiles, 256, 0, s>>>(nodes, tiles, P->posP, P->posQ, P->res[cur], P->xs, P->ys, P->tab,
                                                    P->vec, d_err);
             sa_scan_kernel<<<L.nl0, 256, 0, s>>>(nodes, P->d_tasks + L.o_l0, P->tab, P->vec, 0);
-            sa_scan_kernel<<<L.nl1, 256, 0, s>>>(nodes, P->d_tasks + L.o_l1, P->tab, P->vec, 1);
+            sa_scan_cols_kernel<<<L.nl1, 256, 0, s>>>(nodes, P->d_tasks + L.o_l1, P->tab);
             if (L.nct)
                 sa_coarse_kernel<<<(L.nct + 7) / 8, 256, 0, s>>>(nodes, P->d_tasks + L.o_ct, L.nct, P->tab, P->vec,
                                                                  P->ys, P->cst);
