@@ -49,6 +49,7 @@ struct SaShared {
     uint16_t xs[kSaSB];   // node-local row -> col | hi << 15
     uint16_t ys[kSaSB];   // node-local col -> row | hi << 15
     int32_t cst[kSaSB / kSaSF + 8];    // c* at node row R, slot (node start + R) / kSaSF
+    int32_t sub[kSaSB / kSaSC];        // lo rows per kSaSC-row sub-band of the block (coarse phase)
 };
 static_assert(kSaSB / kSaSF <= kSaThreads - 32, "phase C needs at least one warp without a thread walk");
 
@@ -249,6 +250,84 @@ __device__ __forceinline__ void warp_walk(SaShared &S, int a, int k, int top, in
     __syncwarp();
 }
 
+// One warp: the levels of spans 2..32 of the 32-leaf group at o (cnt <= 32 leaves), in registers.  Lane i
+// holds element i of the group; per level, every element's parent positions come from counting the smaller
+// elements of the sibling child (shuffles), the children's products are mapped to parent coordinates through
+// the group's slice of xs / ys, c*(r) of each row comes straight from its definition (delta(r, 0) by a ballot,
+// then one pass over the node's columns), and the lists are reordered through the group's slice of PL / QL.
+// Only __syncwarp: nothing here is shared with other warps.
+__device__ __forceinline__ void warp_low_levels(SaShared &S, int o, int cnt, int lane) {
+    int pl = lane < cnt ? S.PL[o + lane] : INT_MAX;
+    int ql = lane < cnt ? S.QL[o + lane] : INT_MAX;
+    int res = 0;
+    for (int h = 1; h < 32 && h < cnt; h <<= 1) {
+        const int s = 2 * h;
+        const int a = lane & ~(s - 1);
+        const int m = min(a + h, cnt), b = min(a + s, cnt);
+        const bool two = lane < cnt && m < b;   // the lane's node has both children
+        const bool lo = lane < m;
+        // parent positions in the row-id (PL) and column-id (QL) merges
+        const int sb = lo ? m : a, se = lo ? b : m;
+        int cp = 0, cq = 0;
+        for (int t = 0; t < h; ++t) {
+            const int src = (sb + t) & 31;
+            const int vp = __shfl_sync(kFull, pl, src);
+            const int vq = __shfl_sync(kFull, ql, src);
+            if (sb + t < se) {
+                cp += vp < pl;
+                cq += vq < ql;
+            }
+        }
+        const int base = lo ? lane - a : lane - m;
+        const int pp = two ? base + cp : lane - a;
+        const int pq = two ? base + cq : lane - a;
+        // the child's product (row -> child-local col) in the parent's coordinates
+        const int cs = lo ? a : m;
+        const int col = __shfl_sync(kFull, pq, (cs + res) & 31);
+        if (two) {
+            S.xs[o + a + pp] = (uint16_t) (col | (lo ? 0 : 0x8000));
+            S.ys[o + a + col] = (uint16_t) (pp | (lo ? 0 : 0x8000));
+        }
+        __syncwarp();
+        const int x = two ? S.xs[o + lane] : 0;
+        const int y = two ? S.ys[o + lane] : 0;
+        // c*(r) = min{c : delta(r, c) >= 0}, delta(r, 0) = -#{lo points in rows >= r}
+        const int k = b - a, r = lane - a;
+        const unsigned lomask = __ballot_sync(kFull, two && !(x >> 15));
+        const unsigned upto = b >= 32 ? 0xffffffffu : ((1u << b) - 1u);
+        int delta = -__popc(lomask & upto & ~((1u << lane) - 1u));
+        int cstar = delta >= 0 ? 0 : k + 1;
+        for (int c = 0; c < s; ++c) {
+            const int yc = __shfl_sync(kFull, y, (a + c) & 31);
+            if (c < k && cstar > k) {
+                const int yr = yc & 0x7fff;
+                delta += (yc >> 15) ? (yr < r) : (yr >= r);
+                if (delta >= 0) cstar = c + 1;
+            }
+        }
+        if (two) {
+            const int xr = x & 0x7fff;
+            const bool hi = x >> 15;
+            const bool good = cstar >= 1 && cstar <= k && (hi ? (xr < cstar) : (xr >= cstar));
+            res = good ? cstar - 1 : xr;
+        }
+        // the lists in the parent's order
+        __syncwarp();
+        if (two) {
+            S.PL[o + a + pp] = pl;
+            S.QL[o + a + pq] = ql;
+        }
+        __syncwarp();
+        if (two) {
+            pl = S.PL[o + lane];
+            ql = S.QL[o + lane];
+        }
+        __syncwarp();
+    }
+    if (lane < cnt) S.RES[o + lane] = (uint16_t) res;
+    __syncwarp();
+}
+
 __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *__restrict__ Pinv,
                                                              const int32_t *__restrict__ Q,
                                                              const SaBlockItem *__restrict__ items,
@@ -265,7 +344,10 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
         S.RES[e] = 0;
     }
     __syncthreads();
-    for (int size = 1; size < nb; size <<= 1) {
+    // spans 2..32: one warp per 32-leaf group
+    for (int o = warp * 32; o < nb; o += nwarps * 32) warp_low_levels(S, o, min(32, nb - o), lane);
+    __syncthreads();
+    for (int size = 32; size < nb; size <<= 1) {
         const int span = size << 1;
         // ---- merge the children's lists: positions in the parent lists ----
         if (span >= 2 * kSaPerThread) {
@@ -347,7 +429,19 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
         const int rem = nb - nfull * span;            // size of the trailing node
         const int nnodes = nfull + (rem > size ? 1 : 0);
         if (span > kSaSF) {
-            // phase A: coarse boundaries (multiples of kSaSC inside each node), full scans
+            // phase A: coarse boundaries (multiples of kSaSC inside each node).  c*(R) is the need-th column
+            // raising delta in row R, need = the lo rows at or below R: counted once per kSaSC-row sub-band (warp
+            // w: block rows [w kSaSC, (w+1) kSaSC), inside one node) and summed per boundary.
+            if (warp * kSaSC < nb) {
+                const int r0 = warp * kSaSC, r1 = min(r0 + kSaSC, nb);
+                int cnt = 0;
+                for (int r = r0; r < r1; r += 32) {
+                    const int rr = r + lane;
+                    cnt += __popc(__ballot_sync(kFull, rr < r1 && !(S.xs[rr] >> 15)));
+                }
+                if (lane == 0) S.sub[warp] = cnt;
+            }
+            __syncthreads();
             const int ca_full = (span - 1) / kSaSC;
             const int ca_last = rem > size ? (rem - 1) / kSaSC : 0;
             for (int t = warp; t < nfull * ca_full + ca_last; t += nwarps) {
@@ -355,7 +449,8 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
                 task_node(t, ca_full, nfull, nd, jj);
                 const int a = nd * span, k = nd < nfull ? span : rem;
                 const int R = (jj + 1) * kSaSC;
-                const int need = warp_row_count(S, a, R, k, 0, lane);   // lo rows at or below R
+                int need = 0;   // lo rows at or below R
+                for (int w = (a + R) / kSaSC; w * kSaSC < a + k; ++w) need += S.sub[w];
                 const int cst = warp_col_search(S, a, k, 0, need, R, lane);
                 if (lane == 0) S.cst[(a + R) / kSaSF] = cst;
             }
