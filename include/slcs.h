@@ -146,6 +146,13 @@ int slcs_scores(const int32_t *row_to_col, int m, int n, const slcs_query *q, in
 int slcs_scores_dev(const int32_t *d_row_to_col, int m, int n, const slcs_query *d_q, int nq, int32_t *d_out,
                     void *stream);
 
+/* Window scan: out[s] = LCS(a, b[s..s+w)) for every s = 0..n-w (n-w+1 values), in O(m+n) for all windows:
+ * the incremental dominance moves of the reference's window matcher (R:approximate_matching/WindowAMatch.h:
+ * 26-71) as one prefix sum.  The _dev form takes an optional col_to_row (NULL: computed on the device). */
+int slcs_window_scores(const int32_t *row_to_col, int m, int n, int w, int32_t *out);
+int slcs_window_scores_dev(const int32_t *d_row_to_col, const int32_t *d_col_to_row, int m, int n, int w,
+                           int32_t *d_out, void *stream);
+
 /* ---- batched combing -------------------------------------------------------------------------- */
 /* Braids of npairs independent pairs in one persistent, length-bucketed launch.  a_cat / b_cat hold the
  * concatenated symbols, a_off / b_off (npairs) the start of each string, m / n (npairs) the lengths;
@@ -235,6 +242,8 @@ int slcs_server_submit(slcs_server *srv, const uint8_t *a, int m, const uint8_t 
 int slcs_server_poll(slcs_server *srv, slcs_result *out, int cap, int *count, int timeout_ms);
 /* More queries on a finished request's resident braid (synchronous). */
 int slcs_server_query(slcs_server *srv, uint64_t ticket, const slcs_query *q, int nq, int32_t *out);
+/* Window scan of a resident braid: out[s] = LCS(a, b[s..s+w)), s = 0..n-w (synchronous). */
+int slcs_server_window(slcs_server *srv, uint64_t ticket, int w, int32_t *out);
 /* Copies a resident braid (row_to_col, m+n entries) to the host. */
 int slcs_server_braid(slcs_server *srv, uint64_t ticket, int32_t *row_to_col);
 int slcs_server_release(slcs_server *srv, uint64_t ticket);

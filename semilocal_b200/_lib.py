@@ -117,6 +117,9 @@ SIGNATURES = {
     "slcs_server_release": [_vp, ctypes.c_uint64],
     "slcs_server_stats_get": [_vp, ctypes.POINTER(ServerStats)],
     "slcs_server_destroy": [_vp],
+    "slcs_window_scores": [_i32p, _int, _int, _int, _i32p],
+    "slcs_window_scores_dev": [_vp, _vp, _int, _int, _int, _vp, _vp],
+    "slcs_server_window": [_vp, ctypes.c_uint64, _int, _i32p],
     "slcs_autotune": [_int, ctypes.POINTER(Tuning)],
     "slcs_tuning_get": [ctypes.POINTER(Tuning)],
     "slcs_tuning_set": [ctypes.POINTER(Tuning)],

@@ -127,6 +127,14 @@ def staggered_glue(p, pm: int, pn: int, q, qm: int, qn: int, row_glue: bool) -> 
     return out
 
 
+def window_scores(row_to_col, m: int, n: int, w: int) -> np.ndarray:
+    """LCS(a, b[s..s+w)) for every window s = 0..n-w, read from the braid in one pass on the device."""
+    r2c = np.ascontiguousarray(row_to_col, dtype=np.int32)
+    out = np.empty(max(n - w + 1, 1), dtype=np.int32)
+    check(lib().slcs_window_scores(_p(r2c, _i32p), m, n, w, _p(out, _i32p)))
+    return out[:max(n - w + 1, 0)]
+
+
 def scores(row_to_col, m: int, n: int, queries: Sequence[Tuple[int, int, int]]) -> np.ndarray:
     """Answer (kind, i, j) queries against a braid; see SLCS_Q_* in include/slcs.h."""
     r2c = np.ascontiguousarray(row_to_col, dtype=np.int32)
@@ -360,6 +368,13 @@ class Server:
         out = np.zeros(len(queries), np.int32)
         _lib.check(_lib.lib().slcs_server_query(self._h, ticket, qs, len(queries), _p(out, _i32p)))
         return out
+
+    def window_scores(self, ticket: int, w: int) -> np.ndarray:
+        """LCS(a, b[s..s+w)) for every window of the resident braid of `ticket`."""
+        m, n = self._sizes[ticket]
+        out = np.zeros(max(n - w + 1, 1), np.int32)
+        _lib.check(_lib.lib().slcs_server_window(self._h, ticket, w, _p(out, _i32p)))
+        return out[:max(n - w + 1, 0)]
 
     def braid(self, ticket: int) -> np.ndarray:
         m, n = self._sizes[ticket]

@@ -656,6 +656,35 @@ int slcs_server_braid(slcs_server *S, uint64_t ticket, int32_t *row_to_col) {
     return rc;
 }
 
+int slcs_server_window(slcs_server *S, uint64_t ticket, int w, int32_t *out) {
+    if (!S || !out) return fail(SLCS_ERR_ARG, "bad arguments");
+    Resident R;
+    {
+        std::lock_guard<std::mutex> lk(S->rmu);
+        auto it = S->resident.find(ticket);
+        if (it == S->resident.end()) return fail(SLCS_ERR_ARG, "braid not resident (unknown, pending, released or evicted)");
+        it->second.pins++;
+        it->second.lru = ++S->lru_clock;
+        R = it->second;
+    }
+    int rc = SLCS_OK;
+    if (w < 1 || w > R.n) rc = fail(SLCS_ERR_ARG, "window length must be in [1, n]");
+    if (rc == SLCS_OK) {
+        std::lock_guard<std::mutex> lk(S->qmu);
+        DevBuf<int32_t> dout;
+        rc = dout.alloc(R.n - w + 1, S->qstream);
+        if (rc == SLCS_OK) rc = window_scores_dev(R.r2c, nullptr, R.m, R.n, w, dout.p, S->qstream);
+        if (rc == SLCS_OK &&
+            (cudaMemcpyAsync(out, dout.p, sizeof(int32_t) * (size_t) (R.n - w + 1), cudaMemcpyDeviceToHost,
+                             S->qstream) != cudaSuccess ||
+             cudaStreamSynchronize(S->qstream) != cudaSuccess))
+            rc = fail(SLCS_ERR_CUDA, "window download failed");
+    }
+    std::lock_guard<std::mutex> lk(S->rmu);
+    S->resident[ticket].pins--;
+    return rc;
+}
+
 int slcs_server_release(slcs_server *S, uint64_t ticket) {
     if (!S) return fail(SLCS_ERR_ARG, "NULL server");
     std::lock_guard<std::mutex> lk(S->rmu);

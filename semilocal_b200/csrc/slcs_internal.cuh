@@ -239,6 +239,8 @@ __device__ __forceinline__ void query_to_matrix(const slcs_query &q, int m, int 
 
 int launch_scores(const int32_t *d_r2c, int m, int n, const slcs_query *d_q, int nq, int32_t *d_out, int *d_err,
                   cudaStream_t s);
+// LCS(a, b[s..s+w)) for every window s = 0..n-w of a braid (d_c2r optional: computed when NULL); synchronous.
+int window_scores_dev(const int32_t *d_r2c, const int32_t *d_c2r, int m, int n, int w, int32_t *d_out, cudaStream_t s);
 // The same for host queries / answers (synchronous on s).
 int launch_scores_host(const int32_t *d_r2c, int m, int n, const slcs_query *q, int nq, int32_t *out,
                        cudaStream_t s);

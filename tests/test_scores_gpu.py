@@ -41,3 +41,22 @@ def test_out_of_range_query_is_an_error(engine):
     r2c, _ = engine.comb(np.array([1, 2], np.uint8), np.array([2, 1], np.uint8))
     with pytest.raises(engine.SlcsError):
         engine.scores(r2c, 2, 2, [(engine.Q_STRING_SUBSTRING, 2, 1)])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("m,n,w", [(1, 1, 1), (5, 9, 3), (300, 200, 1), (300, 200, 200), (700, 1000, 64),
+                                   (1200, 5000, 777), (50, 4200, 2049)])
+def test_window_scores_match_dp(engine, oracle, m, n, w):
+    import semilocal_b200 as S
+    from semilocal_b200 import gen
+    a = gen.uniform_string(m, 4, 70 + m, 1)
+    b = gen.uniform_string(n, 4, 80 + n, 2)
+    braid = oracle.comb_antidiag(a, b)
+    got = S.window_scores(braid, m, n, w)
+    assert len(got) == n - w + 1
+    step = max(1, (n - w + 1) // 64)   # the DP per window is O(m w): check a spread of windows, and the last
+    for s in list(range(0, n - w + 1, step)) + [n - w]:
+        assert int(got[s]) == oracle.lcs_dp(a, b[s:s + w]), (s, w)
+    # every window against the braid's own string-substring queries
+    qs = [(S.Q_STRING_SUBSTRING, s, s + w) for s in range(n - w + 1)]
+    assert np.array_equal(got, S.scores(braid, m, n, qs))

@@ -124,6 +124,10 @@ def test_server_resident_queries_and_release(engine):
         qs = [_random_query(rng, len(a), len(b)) for _ in range(20)]
         out = srv.query(t, qs)
         assert [int(x) for x in out] == [_expected(a, b, q) for q in qs]
+        win = srv.window_scores(t, 150)
+        assert len(win) == len(b) - 150 + 1
+        for s0 in (0, 1, 500, len(b) - 150):
+            assert int(win[s0]) == O.lcs_dp(a, b[s0:s0 + 150])
         srv.release(t)
         with pytest.raises(S.SlcsError):
             srv.query(t, [(0, 0, 0)])
