@@ -47,8 +47,11 @@ constexpr int kChunk = 16;   // hand-off words between bands are published / pol
 // strip r-1's bottom row (so the RS strips of a lane update independently every step); lanes are RS+1 blocks
 // apart and hand one 32-bit word per block to the next lane by shuffle.  Strips outside their real blocks keep
 // running on padding columns, whose "outside" plane forces non-matches, so the loop has no per-strip branches.
+constexpr int kRing = 256;   // column-plane words a warp keeps in shared memory (a ring, index & 255)
+
 template <int RS>
-__device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int *err, int lane) {
+__device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int *err, int lane,
+                                         uint32_t (*ring)[kRing]) {
     uint32_t A1[RS], A0[RS], L[RS], T[RS], V[RS];
     bool live[RS];
 #pragma unroll
@@ -67,18 +70,48 @@ __device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int
     const int gmax = 31 * (RS + 1) + RS - 1 + nb;
     uint32_t carry = 0u;    // input word of strip 0, from the lane above (previous iteration)
     uint32_t chunkw = 0u;   // lanes 0..kChunk-1: the current chunk of hand-off words from the band above
+    // Column-plane words (index 0 .. nb + 2) reach the lanes through a ring in shared memory: the warp loads
+    // 32 words per plane every 32 iterations, 64 words ahead, and stores them one iteration later, so no load
+    // latency sits on the loop.  At iteration g the lanes read words >= g - 31 (RS + 1) - RS + 1 and <= g + 3;
+    // the ring then holds words [g - 161, g + 94] (RS <= 4), so nothing live is overwritten.
+    const int last = nb + 2;
+    __syncwarp();
+    for (int idx = lane; idx < 64; idx += 32)
+        if (idx <= last) {
+            ring[0][idx & (kRing - 1)] = __ldg(P.b1 + idx);
+            ring[1][idx & (kRing - 1)] = __ldg(P.b0 + idx);
+            ring[2][idx & (kRing - 1)] = __ldg(P.b2 + idx);
+        }
+    __syncwarp();
+    uint32_t s1 = 0u, s0 = 0u, s2 = 0u;   // words loaded at g % 32 == 0, stored at g % 32 == 1
     uint32_t p1[RS], pl1[RS], p0[RS], pl0[RS], p2[RS], pl2[RS];   // plane words of the next iteration
 #pragma unroll
     for (int r = 0; r < RS; ++r) {
         const int q = min(max(-lag - r, -1), nb);
-        p1[r] = __ldg(P.b1 + q + 1);
-        pl1[r] = __ldg(P.b1 + q + 2);
-        p0[r] = __ldg(P.b0 + q + 1);
-        pl0[r] = __ldg(P.b0 + q + 2);
-        p2[r] = __ldg(P.b2 + q + 1);
-        pl2[r] = __ldg(P.b2 + q + 2);
+        p1[r] = ring[0][(q + 1) & (kRing - 1)];
+        pl1[r] = ring[0][(q + 2) & (kRing - 1)];
+        p0[r] = ring[1][(q + 1) & (kRing - 1)];
+        pl0[r] = ring[1][(q + 2) & (kRing - 1)];
+        p2[r] = ring[2][(q + 1) & (kRing - 1)];
+        pl2[r] = ring[2][(q + 2) & (kRing - 1)];
     }
     for (int g = 0; g < gmax; ++g) {
+        if ((g & 31) == 1) {
+            const int idx = g - 1 + 64 + lane;
+            if (idx <= last) {
+                ring[0][idx & (kRing - 1)] = s1;
+                ring[1][idx & (kRing - 1)] = s0;
+                ring[2][idx & (kRing - 1)] = s2;
+            }
+            __syncwarp();
+        } else if ((g & 31) == 0) {
+            const int idx = g + 64 + lane;
+            if (idx <= last) {
+                s1 = __ldg(P.b1 + idx);
+                s0 = __ldg(P.b0 + idx);
+                s2 = __ldg(P.b2 + idx);
+            }
+        }
         // lane 0's input word: from the band above (zero strands for the first band).  The band above is
         // polled once per kChunk words; the chunk's words are then loaded by lanes 0..kChunk-1 in one go and
         // handed to lane 0 by shuffle, one per iteration.
@@ -97,12 +130,12 @@ __device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int
         for (int r = 0; r < RS; ++r) {
             h1[r] = p1[r]; l1[r] = pl1[r]; h0[r] = p0[r]; l0[r] = pl0[r]; h2[r] = p2[r]; l2[r] = pl2[r];
             const int q = min(max(g + 1 - lag - r, -1), nb);
-            p1[r] = __ldg(P.b1 + q + 1);
-            pl1[r] = __ldg(P.b1 + q + 2);
-            p0[r] = __ldg(P.b0 + q + 1);
-            pl0[r] = __ldg(P.b0 + q + 2);
-            p2[r] = __ldg(P.b2 + q + 1);
-            pl2[r] = __ldg(P.b2 + q + 2);
+            p1[r] = ring[0][(q + 1) & (kRing - 1)];
+            pl1[r] = ring[0][(q + 2) & (kRing - 1)];
+            p0[r] = ring[1][(q + 1) & (kRing - 1)];
+            pl0[r] = ring[1][(q + 2) & (kRing - 1)];
+            p2[r] = ring[2][(q + 1) & (kRing - 1)];
+            pl2[r] = ring[2][(q + 2) & (kRing - 1)];
         }
         uint32_t out = 0u;
 #pragma unroll
@@ -149,13 +182,14 @@ template <int RS>
 __global__ void __launch_bounds__(32) bit_kernel(const BitPair *__restrict__ pairs, const BitItem *__restrict__ items,
                                                   int nitems, int *next, int *err) {
     const int lane = threadIdx.x & 31;
+    __shared__ uint32_t ring[3][kRing];
     for (;;) {
         int it = nitems;
         if (lane == 0 && ld_relaxed(err) == kDevErrNone) it = atomicAdd(next, 1);
         it = __shfl_sync(kFull, it, 0);
         if (it >= nitems) return;
         const BitItem I = items[it];
-        bit_band<RS>(pairs[I.pair], I, err, lane);
+        bit_band<RS>(pairs[I.pair], I, err, lane, ring);
     }
 }
 
