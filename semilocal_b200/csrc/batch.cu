@@ -140,7 +140,14 @@ int slcs_batch_create(const int32_t *m, const int32_t *n, int npairs, int mode, 
             if (mode == 1) bt->item_begin.push_back((int) bt->items.size());
         }
     }
-    if (mode == 0) bt->item_begin.push_back((int) bt->items.size());
+    if (mode == 0) {
+        // band-major order (all first bands by decreasing pair cost, then all second bands, ...): a warp takes
+        // band k of a pair only after band k-1 of it is well under way, instead of idling behind it.  A band still
+        // waits only on a band taken earlier, so no assumption about co-residency is added.
+        std::stable_sort(bt->items.begin(), bt->items.end(),
+                         [](const CombItem &x, const CombItem &y) { return x.band < y.band; });
+        bt->item_begin.push_back((int) bt->items.size());
+    }
     bt->resident = comb_resident_warps(E);
     cudaStream_t s = E->stream;
     auto cleanup_fail = [&](int rc) {
@@ -210,13 +217,10 @@ int slcs_batch_upload(slcs_batch *bt, const uint8_t *a_cat, const int64_t *a_off
     bool same = bt->pairs_ready;
     for (int i = 0; i < np && same; ++i) same = bt->a_off[i] == a_off[i] && bt->b_off[i] == b_off[i];
     if (!same) {
-        // one progress slot per item (band), in plan order: a pair's slots start at its first band's item
-        std::vector<int64_t> prog_off(np, 0);
-        int64_t acc = 0;
-        for (const CombItem &it : bt->items) {
-            if (it.band == 0) prog_off[it.pair] = acc;
-            acc++;
-        }
+        // one progress slot per band: pair p's slots are a contiguous range (whatever the items' order)
+        std::vector<int64_t> prog_off(np + 1, 0);
+        for (const CombItem &it : bt->items) prog_off[it.pair + 1]++;
+        for (int p = 0; p < np; ++p) prog_off[p + 1] += prog_off[p];
         std::vector<CombPair> hp(np);
         for (int p = 0; p < np; ++p)
             hp[p] = CombPair{bt->da + a_off[p], bt->db + b_off[p], bt->dc2r + bt->out_off[p], bt->dprog + prog_off[p],
