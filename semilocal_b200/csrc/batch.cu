@@ -136,7 +136,9 @@ int slcs_batch_create(const int32_t *m, const int32_t *n, int npairs, int mode, 
     for (int oi = 0; oi < npairs; ++oi) {
         const int p = order[oi];
         if (m[p] > 0 && n[p] > 0) {
-            bt->prog_total += plan_bands(p, m[p], Rforce ? Rforce : pick_rows_batch(m[p]), bt->items);
+            // mode 1 launches every pair alone, so it takes the band height tuned for a lone pair
+            const int R = Rforce ? Rforce : (mode == 1 ? pick_rows_single(m[p]) : pick_rows_batch(m[p]));
+            bt->prog_total += plan_bands(p, m[p], R, bt->items);
             if (mode == 1) bt->item_begin.push_back((int) bt->items.size());
         }
     }

@@ -171,6 +171,7 @@ struct HybridPlan {
     int64_t tile_total = 0;
     // tiles
     std::vector<CombItem> items;
+    std::vector<int> prog_first;   // tile t's progress slots start here
     CombPair *d_pairs = nullptr;
     CombItem *d_items = nullptr;
     int64_t *d_tile_off = nullptr;
@@ -260,6 +261,12 @@ int hybrid_plan_create(int m, int n, int tile_rows, int tile_cols, Engine *E, cu
         nprog += plan_bands((int) t, cur[t].m, pick_rows_batch(cur[t].m), H->items);
     }
     H->nprog = nprog;
+    // band-major order: a tile's band k is taken once its band k-1 is under way (progress slots do not depend
+    // on the order: tile t's slots start at the number of bands of the tiles before it)
+    H->prog_first.assign(cur.size() + 1, 0);
+    for (const CombItem &it : H->items) H->prog_first[it.pair + 1]++;
+    for (size_t t = 0; t < cur.size(); ++t) H->prog_first[t + 1] += H->prog_first[t];
+    std::stable_sort(H->items.begin(), H->items.end(), [](const CombItem &x, const CombItem &y) { return x.band < y.band; });
     H->resident = comb_resident_warps(E);
     // reduction schedule (R:include/SemiLocal/SemiLocalLCS.h:708-789)
     int smallM = H->M, smallN = H->N;
@@ -399,9 +406,8 @@ int hybrid_plan_run(HybridPlan *H, const T *d_a, const T *d_b, int *d_err, cudaS
             hp[t].c2r = H->c2r[0] + acc;
             acc += hp[t].m + hp[t].n;
         }
-        // one progress slot per item; a tile's bands are consecutive items, band 0 first
-        for (size_t x = 0; x < H->items.size(); ++x)
-            if (H->items[x].band == 0) hp[H->items[x].pair].progress = H->d_prog + x;
+        // one progress slot per band; tile t's slots start at prog_first[t]
+        for (size_t t = 0; t < hp.size(); ++t) hp[t].progress = H->d_prog + H->prog_first[t];
         SLCS_CUDA_TRY(cudaMemcpyAsync(H->d_pairs, hp.data(), sizeof(CombPair) * hp.size(), cudaMemcpyHostToDevice, s));
         SLCS_CUDA_TRY(cudaStreamSynchronize(s));
         H->bound_a = d_a;

@@ -285,6 +285,8 @@ int launch_group(slcs_server *S, int idx, std::vector<Req *> &reqs, int warp_cap
         if (r->m > 0 && r->n > 0) nb = plan_bands(i, r->m, r->R, items);
         prog_off[i + 1] = prog_off[i] + nb;
     }
+    // band-major order: a request's band k is taken once its band k-1 is under way (slots are per request)
+    std::stable_sort(items.begin(), items.end(), [](const CombItem &x, const CombItem &y) { return x.band < y.band; });
     const int ni = (int) items.size();
     // meta layout
     size_t off = 0;
