@@ -4,8 +4,9 @@
 // a worker thread owned by the server
 //   * admits them by a device-memory budget (inputs, strands and scratch while in flight, the braid while
 //     resident), evicting least recently used resident braids when the budget is short;
-//   * launches admitted requests as soon as a stream is free: requests of at least big_cells cells run alone
-//     on one of the big streams (two by default), the others are batched (largest first) into one persistent
+//   * launches admitted requests as soon as a stream is free: requests of at least big_cells cells run on one
+//     of the big streams (two by default; alone, or with other pending big requests when several wait), the
+//     others are batched (largest first) into one persistent
 //     combing launch on one of the small streams.  Each launch caps its persistent grid (big: half the
 //     resident warps, small: a quarter), so long big launches leave SMs to the small batches and their work
 //     overlaps on the device; requests that arrive while launches run are admitted into the next launch of a
@@ -421,20 +422,29 @@ bool schedule(slcs_server *S) {
     bool did = false;
     const int W = S->resident_warps;
     auto big = [&](const Req *r) { return r->cells >= S->o.big_cells; };
-    // big streams: the oldest big request that fits, one per free big stream
-    for (int idx = 0; idx < S->nbig; ++idx) {
+    // big streams: the oldest big requests that fit; when several are pending each free big stream takes its
+    // share (at most 8) in one launch, whose band-major work order keeps the device busy across them
+    int pending_big = 0;
+    for (const Req *r : S->pending) pending_big += big(r);
+    for (int idx = 0; idx < S->nbig && pending_big > 0; ++idx) {
         if (S->inflight[idx]) continue;
-        bool launched = false;
-        for (auto it = S->pending.begin(); it != S->pending.end(); ++it) {
-            if (!big(*it)) continue;
+        int free_big = 0;
+        for (int j = idx; j < S->nbig; ++j) free_big += S->inflight[j] == nullptr;
+        const int share = std::min(8, std::max(1, (pending_big + free_big - 1) / free_big));
+        std::vector<Req *> g;
+        for (auto it = S->pending.begin(); it != S->pending.end() && (int) g.size() < share;) {
+            if (!big(*it)) {
+                ++it;
+                continue;
+            }
             if (!reserve(S, (*it)->need, S->streams[idx])) break;
-            std::vector<Req *> g{*it};
-            S->pending.erase(it);
-            launch_group(S, idx, g, S->o.big_warps > 0 ? S->o.big_warps : W / 2);
-            did = launched = true;
-            break;
+            g.push_back(*it);
+            it = S->pending.erase(it);
         }
-        if (!launched) break;
+        if (g.empty()) break;
+        pending_big -= (int) g.size();
+        launch_group(S, idx, g, S->o.big_warps > 0 ? S->o.big_warps : W / 2);
+        did = true;
     }
     // small streams: everything small that fits, oldest first, up to max_batch per launch
     for (size_t idx = S->nbig; idx < S->streams.size(); ++idx) {
