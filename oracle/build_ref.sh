@@ -22,6 +22,12 @@ mkdir -p "$here/_ref"
   -I"$src" "$here/ref_shim.cpp" -o "$here/_ref/libslcs_ref.so.tmp" -Wl,--no-undefined
 mv "$here/_ref/libslcs_ref.so.tmp" "$here/_ref/libslcs_ref.so"
 echo "build_ref: wrote $here/_ref/libslcs_ref.so"
+# Two of the reference's own benchmark executables (its harness protocol: R:utils/runners.py), as the pin of the
+# harness runners in semilocal_b200/harness/.
+for f in semi_local_naive_iterative semi_local_hybrid_iterative; do
+  /usr/bin/g++ -std=c++17 -O2 -march=x86-64-v3 -fopenmp -w -I"$src" "$src/cpu_impl/$f.cpp" -o "$here/_ref/ref_$f"
+done
+echo "build_ref: wrote the reference runners"
 # The reference's own strategies with the GPU engine plugged in through include/slcs.hpp (needs the engine).
 repo="$(cd "$here/.." && pwd)"
 if [ -f "$repo/semilocal_b200/libslcs.so" ]; then

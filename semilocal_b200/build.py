@@ -61,7 +61,18 @@ def build(verbose: bool = False, force: bool = False, extra=None) -> str:
     cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
+    build_runners()
     return LIB
+
+
+def build_runners() -> None:
+    """The harness executables (semilocal_b200/harness/): combing (braid hash) and LCS (score)."""
+    src = os.path.join(HERE, "harness", "slcs_runner.cpp")
+    inc = os.path.join(HERE, "..", "include")
+    for name, defs in (("slcs_comb_runner", []), ("slcs_lcs_runner", ["-DSLCS_RUNNER_LCS"])):
+        out = os.path.join(HERE, "harness", name)
+        subprocess.run(["g++", "-std=c++17", "-O2", *defs, "-I", inc, src, "-L", HERE, "-lslcs",
+                        "-Wl,-rpath,$ORIGIN/..", "-o", out], check=True)
 
 
 if __name__ == "__main__":
