@@ -274,6 +274,16 @@ int slcs_autotune(int flags, slcs_tuning *out);
 int slcs_tuning_get(slcs_tuning *out);
 int slcs_tuning_set(const slcs_tuning *in);
 
+/* ---- failure-path self-test (no counterpart in the reference) ------------------------------------ */
+/* Runs the combing kernel on a band whose upstream band is never launched, so its bounded wait (about 2 s of
+ * the GPU timer) gives up: *status receives the status the engine reports for it (SLCS_ERR_TIMEOUT when the
+ * failure path works).  Nothing faults; the engine stays usable.  Returns SLCS_OK if the test could run. */
+int slcs_selftest_wait_timeout(int32_t *status);
+/* Debug check of a braid or product (no counterpart in the reference): every entry of perm[0..size) is in range
+ * and no value repeats.  SLCS_OK if so, else SLCS_ERR_INTERNAL; *bad_entries (optional) counts the offenders. */
+int slcs_check_permutation(const int32_t *perm, int size, int32_t *bad_entries);
+int slcs_check_permutation_dev(const int32_t *d_perm, int size, int32_t *bad_entries, void *stream);
+
 /* ---- measurement helper (no counterpart in the reference) --------------------------------------- */
 /* Issue-rate ceiling of the combing cell's instruction mix on this device, in cells per second
  * (independent cells at full occupancy): the denominator of the combing kernels' roofline fraction. */

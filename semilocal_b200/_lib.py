@@ -120,6 +120,9 @@ SIGNATURES = {
     "slcs_window_scores": [_i32p, _int, _int, _int, _i32p],
     "slcs_window_scores_dev": [_vp, _vp, _int, _int, _int, _vp, _vp],
     "slcs_server_window": [_vp, ctypes.c_uint64, _int, _i32p],
+    "slcs_selftest_wait_timeout": [_i32p],
+    "slcs_check_permutation": [_i32p, _int, _i32p],
+    "slcs_check_permutation_dev": [_vp, _int, _i32p, _vp],
     "slcs_autotune": [_int, ctypes.POINTER(Tuning)],
     "slcs_tuning_get": [ctypes.POINTER(Tuning)],
     "slcs_tuning_set": [ctypes.POINTER(Tuning)],

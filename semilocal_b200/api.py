@@ -127,6 +127,16 @@ def staggered_glue(p, pm: int, pn: int, q, qm: int, qn: int, row_glue: bool) -> 
     return out
 
 
+def check_permutation(perm) -> int:
+    """Number of entries of `perm` that are out of range or repeat a value (0 for a permutation), on the GPU."""
+    p = np.ascontiguousarray(perm, dtype=np.int32)
+    bad = ctypes.c_int32(0)
+    rc = lib().slcs_check_permutation(_p(p, _i32p), len(p), ctypes.byref(bad))
+    if rc not in (0, 7):
+        check(rc)
+    return int(bad.value)
+
+
 def window_scores(row_to_col, m: int, n: int, w: int) -> np.ndarray:
     """LCS(a, b[s..s+w)) for every window s = 0..n-w, read from the braid in one pass on the device."""
     r2c = np.ascontiguousarray(row_to_col, dtype=np.int32)

@@ -72,6 +72,7 @@ struct slcs_batch {
 namespace {
 
 int batch_step(slcs_batch *bt, cudaStream_t s, bool capturing) {
+    NvtxRange nv("slcs: batch step");
     // inside a capture the timing events must become external event-record nodes of the graph
     const unsigned evflags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     const int np = bt->npairs;

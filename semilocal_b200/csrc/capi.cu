@@ -160,6 +160,7 @@ bool use_hybrid(const slcs_opts *opts, int m, int n) {
 template <typename T>
 int comb_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int32_t *d_r2c, int32_t *d_c2r, int32_t *d_score,
              const slcs_opts *opts, cudaStream_t s) {
+    NvtxRange nv("slcs: combing");
     if (use_hybrid(opts, m, n)) return comb_hybrid_dev<T>(E, d_a, m, d_b, n, d_r2c, d_c2r, d_score, opts, s);
     return comb_wavefront_dev<T>(E, d_a, m, d_b, n, d_r2c, d_c2r, d_score, opts, s);
 }

@@ -394,6 +394,7 @@ int hybrid_plan_create(int m, int n, int tile_rows, int tile_cols, Engine *E, cu
 // (hybrid_result_r2c, hybrid_result_c2r).
 template <typename T>
 int hybrid_plan_run(HybridPlan *H, const T *d_a, const T *d_b, int *d_err, cudaStream_t s) {
+    NvtxRange nv("slcs: hybrid (tiles + glue tree)");
     if (H->bound_a != d_a || H->bound_b != d_b) {
         // tile descriptors point into the strings: rebuilt when the strings move
         std::vector<CombPair> hp = H->pairs_host;

@@ -180,6 +180,7 @@ __global__ void __launch_bounds__(256) win_out_kernel(const int32_t *__restrict_
 }
 
 int window_scores_dev(const int32_t *d_r2c, const int32_t *d_c2r, int m, int n, int w, int32_t *d_out, cudaStream_t s) {
+    NvtxRange nv("slcs: window scan");
     const int size = m + n, nwin = n - w + 1;
     if (nwin <= 0) return SLCS_OK;
     const int nblk = (nwin + kWinPer - 1) / kWinPer;

@@ -275,6 +275,7 @@ void finish_req(slcs_server *S, Req *r, int status, int32_t score, double t_done
 
 // Builds and enqueues one launch of the requests on stream idx.  Their budget is already reserved.
 int launch_group(slcs_server *S, int idx, std::vector<Req *> &reqs, int warp_cap) {
+    NvtxRange nv("slcs: server launch");
     cudaStream_t s = S->streams[idx];
     std::sort(reqs.begin(), reqs.end(), [](const Req *x, const Req *y) { return x->cells > y->cells; });
     const int np = (int) reqs.size();

@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+
+#include <nvtx3/nvToolsExt.h>
 #include <vector>
 
 #include "../../include/slcs.h"
@@ -20,10 +22,19 @@ constexpr int kDevErrNone = 0;
 constexpr int kDevErrTimeout = 1;     // a bounded spin gave up
 constexpr int kDevErrBadState = 2;    // an internal consistency check failed
 
-// Spin limits: each wait gives up after kSpinLimit polls (sleeping ~kSpinSleepNs between polls), i.e.
-// after a few seconds, sets the error word and returns; waiters also leave as soon as the word is set.
-constexpr long long kSpinLimit = 1ll << 25;
+// Spin limits: each wait gives up after kWaitLimitNs of the GPU's global timer (sleeping ~kSpinSleepNs
+// between polls), sets the error word and returns; waiters also leave as soon as the word is set.  Legitimate
+// waits (a band waiting for the band above it to publish 32 columns) last microseconds.
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 constexpr unsigned kSpinSleepNs = 100;
+
+// NVTX range for the host side of a stage (visible in Nsight timelines; no cost without a tool attached).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // ------------------------------------------------------------------------------------------------
 // host error plumbing
@@ -65,12 +76,23 @@ __device__ __forceinline__ void raise_error(int *err, int code) { atomicCAS(err,
 
 // Wait until *p >= need.  Returns false (after setting *err) when the bounded spin gives up or when
 // another thread already reported an error.  Called by one lane; the caller broadcasts the outcome.
-__device__ __forceinline__ bool wait_at_least(const int *p, int need, int *err) {
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool wait_at_least(const int *p, int need, int *err,
+                                              unsigned long long limit_ns = kWaitLimitNs) {
     if (ld_acquire(p) >= need) return true;
-    for (long long it = 0; it < kSpinLimit; ++it) {
+    const unsigned long long t0 = global_ns();
+    // the iteration cap is a second bound in case the timer does not advance (at >= 100 ns per poll it is
+    // never the first to trigger while the timer runs)
+    for (long long it = 0; it < (1ll << 26); ++it) {
         __nanosleep(kSpinSleepNs);
         if (ld_acquire(p) >= need) return true;
         if (ld_relaxed(err) != kDevErrNone) return false;
+        if (global_ns() - t0 > limit_ns) break;
     }
     raise_error(err, kDevErrTimeout);
     return false;

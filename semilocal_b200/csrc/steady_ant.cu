@@ -1264,6 +1264,7 @@ int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, S
 // the product in root-local coordinates (rank of row id -> rank of column id) to d_R.
 int sa_plan_run_ex(SaPlan *P, const int32_t *d_P, const int32_t *d_leafP, const int32_t *d_Q, int32_t *d_R,
                    int32_t *d_PLout, int32_t *d_QLout, int *d_err, cudaStream_t s) {
+    NvtxRange nv("slcs: steady ant");
     if (P->total == 0) return SLCS_OK;
     const int32_t *leafP = d_leafP;
     if (!leafP) {
