@@ -5,6 +5,7 @@
     python -m semilocal_b200.profile_cases wave   [log2 n]    # wavefront combing of one pair (comb_kernel)
     python -m semilocal_b200.profile_cases hybrid [log2 n]    # hybrid: tile combing + glue tree
     python -m semilocal_b200.profile_cases sa     [log2 n]    # steady ant (sa_* kernels)
+    python -m semilocal_b200.profile_cases probe              # the combing roofline probe (probe_cells_kernel)
 
 Each case runs its plan three times (the first run binds and captures nothing; the runs are plain launches)
 and prints one timing line.  Inputs are the seeded synthetic workloads of semilocal_b200.gen.
@@ -56,6 +57,11 @@ def main(argv):
         dt = (time.perf_counter() - t0) / 3
         pl.check(sh)
         print(f"{case} n=2^{lg} score={int(sc.item())} kernel_ms={pl.kernel_ms():.3f} wall_ms={dt * 1e3:.2f}")
+        return
+    if case == "probe":
+        peak = ctypes.c_double(0)
+        S._lib.check(S.lib().slcs_probe_cell_peak(ctypes.byref(peak)))
+        print(f"probe cells/s={peak.value:.4g}")
         return
     if case == "sa":
         lg = arg or 20
