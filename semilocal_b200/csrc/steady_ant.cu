@@ -17,8 +17,11 @@
 // 1 <= c*(r) <= k and the row's point lies on the wrong side of c*(r) (a hi point left of it or a lo point at
 // or right of it): there the point moves to column c*(r) - 1 (the reference's "good points").  Row by row,
 // c*(r) = c*(r+1) unless row r's point flips the sign, else one past the next column whose point raises
-// delta(r, .).  c* at every 32nd row is found by warp-wide ballot scans; the rows between are walked by one
-// thread each.
+// delta(r, .).  c* at every 32nd row is found by warp-wide ballot scans.  Below 2^12 (shared memory) the rows
+// between are not walked: c* is non-increasing in r and the product is a permutation, so the moving rows take
+// exactly their own columns, the topmost row the largest, and a row moves iff the sign of delta(r, x_r) says
+// so; that sign comes from the c* of the row's 32-row segment and two short counts.  At the HBM levels the rows
+// between are walked by one thread (or, for a long column span, one warp) each.
 #include <algorithm>
 #include <climits>
 #include <numeric>
@@ -33,6 +36,13 @@ constexpr int kSaThreads = 256;
 constexpr int kSaSF = 32;        // rows per walk (fine band)
 constexpr int kSaSC = 512;       // rows per coarse band (full-scan boundaries)
 constexpr int kSaPerThread = kSaSB / kSaThreads;
+constexpr int kSaRankSpan = 1024;  // node spans from which the moving rows are ranked instead of walked
+constexpr int kSegW = kSaSB / 32 / (kSaThreads / 32);   // 32-row segments per warp in the rank passes
+constexpr int kSegB = 8;                                  // segments whose loads a rank pass batches
+static_assert(kSegW % kSegB == 0 && kSegB <= 32, "rank passes take whole batches");
+constexpr int kWalkSpanMax = 64;   // walks crossing more columns are taken by a whole warp
+
+static_assert(kSaSB / kSaSF <= kSaThreads - 32, "the walk phase needs at least one warp without a thread walk");
 
 struct SaBlockItem {
     int64_t off;   // first common index of the block (concatenated problem layout)
@@ -51,7 +61,6 @@ struct SaShared {
     int32_t cst[kSaSB / kSaSF + 8];    // c* at node row R, slot (node start + R) / kSaSF
     int32_t sub[kSaSB / kSaSC];        // lo rows per kSaSC-row sub-band of the block (coarse phase)
 };
-static_assert(kSaSB / kSaSF <= kSaThreads - 32, "phase C needs at least one warp without a thread walk");
 
 __device__ __forceinline__ int count_less(const int32_t *arr, int lo, int hi, int32_t v) {
     // number of entries < v in the sorted range arr[lo, hi)
@@ -64,41 +73,83 @@ __device__ __forceinline__ int count_less(const int32_t *arr, int lo, int hi, in
     return l - lo;
 }
 
-// warp-wide: number of rows r in [r0, r1) of the node at base a whose point raises delta when moving up
-// past it at column c (rowind(r, c) = hi ? x < c : x >= c)
-__device__ __forceinline__ int warp_row_count(const SaShared &S, int a, int r0, int r1, int c, int lane) {
-    int total = 0;
-    for (int r = r0; r < r1; r += 32) {
-        const int rr = r + lane;
-        bool q = false;
-        if (rr < r1) {
-            const int v = S.xs[a + rr];
-            const int x = v & 0x7fff;
-            q = (v >> 15) ? (x < c) : (x >= c);
+// warp-wide: one past the need-th g in [from, end) with pred(g), `none` when there are fewer.  U 32-wide
+// chunks per round: their loads are independent, so a round costs about one load latency (U = 4 for scans that
+// are usually long, 1 for the short ones).
+template <int U, typename Pred>
+__device__ __forceinline__ int ballot_search(int from, int end, int need, int none, int lane, Pred pred) {
+    if (need <= 0) return from;
+    for (int g0 = from; g0 < end; g0 += 32 * U) {
+        bool q[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int g = g0 + 32 * u + lane;
+            q[u] = g < end && pred(g);
         }
-        total += __popc(__ballot_sync(kFull, q));
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const unsigned m = __ballot_sync(kFull, q[u]);
+            const int cnt = __popc(m);
+            if (need <= cnt) return g0 + 32 * u + (int) __fns(m, 0, need) + 1;
+            need -= cnt;
+        }
+    }
+    return none;
+}
+
+// warp-wide: the first i in [l, h) with pred(i), h when there is none (pred monotone: false ... true).  33-way
+// rounds (one probe per lane), so a search over 2^22 entries takes four dependent loads instead of 22.
+template <typename Pred>
+__device__ __forceinline__ int warp_first_true(int l, int h, int lane, Pred pred) {
+    while (h - l > 32) {
+        const int mid = l + (int) (((int64_t) (h - l) * (lane + 1)) / 33);   // strictly increasing probes in [l, h)
+        const int t = __popc(__ballot_sync(kFull, !pred(mid)));              // probes below the answer
+        const int nl = t == 0 ? l : __shfl_sync(kFull, mid, t - 1) + 1;
+        const int nh = t == 32 ? h : __shfl_sync(kFull, mid, t & 31);
+        l = nl;
+        h = nh;
+    }
+    const int i = l + lane;
+    return l + __popc(__ballot_sync(kFull, i < h && !pred(i)));
+}
+
+// warp-wide: #{i in [i0, i1) : pred(i)}, U 32-wide chunks per round
+template <int U, typename Pred>
+__device__ __forceinline__ int ballot_count(int i0, int i1, int lane, Pred pred) {
+    int total = 0;
+    for (int b = i0; b < i1; b += 32 * U) {
+        bool q[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int i = b + 32 * u + lane;
+            q[u] = i < i1 && pred(i);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) total += __popc(__ballot_sync(kFull, q[u]));
     }
     return total;
 }
 
+// warp-wide: number of rows r in [r0, r1) of the node at base a whose point raises delta when moving up
+// past it at column c (rowind(r, c) = hi ? x < c : x >= c)
+template <int U = 1>
+__device__ __forceinline__ int warp_row_count(const SaShared &S, int a, int r0, int r1, int c, int lane) {
+    return ballot_count<U>(r0, r1, lane, [&](int r) {
+        const int v = S.xs[a + r];
+        const int x = v & 0x7fff;
+        return (v >> 15) ? (x < c) : (x >= c);
+    });
+}
+
 // warp-wide: one past the need-th column g >= from whose point raises delta in row R
 // (colind(g, R) = hi ? y < R : y >= R); k + 1 when there is none
+template <int U = 1>
 __device__ __forceinline__ int warp_col_search(const SaShared &S, int a, int k, int from, int need, int R, int lane) {
-    if (need <= 0) return from;
-    for (int g0 = from; g0 < k; g0 += 32) {
-        const int g = g0 + lane;
-        bool q = false;
-        if (g < k) {
-            const int w = S.ys[a + g];
-            const int y = w & 0x7fff;
-            q = (w >> 15) ? (y < R) : (y >= R);
-        }
-        const unsigned mask = __ballot_sync(kFull, q);
-        const int cnt = __popc(mask);
-        if (need <= cnt) return g0 + (int) __fns(mask, 0, need) + 1;
-        need -= cnt;
-    }
-    return k + 1;
+    return ballot_search<U>(from, k, need, k + 1, lane, [&](int g) {
+        const int w = S.ys[a + g];
+        const int y = w & 0x7fff;
+        return (w >> 15) ? (y < R) : (y >= R);
+    });
 }
 
 // flat task index -> (node, task within node); full nodes have per_full tasks, the trailing node the rest
@@ -111,29 +162,6 @@ __device__ __forceinline__ void task_node(int t, int per_full, int nfull, int &n
         jj = t - nfull * per_full;
     }
 }
-
-// one thread: rows [top, bot) of the node at base a, walking up from c = c*(bot)
-__device__ __forceinline__ void thread_walk(SaShared &S, int a, int k, int top, int bot, int c) {
-    for (int r = bot - 1; r >= top; --r) {
-        const int v = S.xs[a + r];
-        const int xr = v & 0x7fff;
-        const bool hi = v >> 15;
-        const bool ind = hi ? (xr < c) : (xr >= c);
-        if (ind) {
-            int g = c;
-            for (; g < k; ++g) {
-                const int w = S.ys[a + g];
-                const int yr = w & 0x7fff;
-                if ((w >> 15) ? (yr < r) : (yr >= r)) break;
-            }
-            c = g < k ? g + 1 : k + 1;
-        }
-        const bool good = c >= 1 && c <= k && (hi ? (xr < c) : (xr >= c));
-        S.RES[a + r] = (uint16_t) (good ? c - 1 : xr);
-    }
-}
-
-constexpr int kWalkSpanMax = 64;   // walks crossing more columns are taken by a whole warp
 
 // one thread: node-local parent positions of the outputs [d, d + cnt) of the merge of the sorted lists
 // L[a, m) (lo child) and L[m, b) (hi child): a merge-path search for the split of the first d outputs, then a
@@ -251,32 +279,34 @@ __device__ __forceinline__ void warp_walk(SaShared &S, int a, int k, int top, in
 }
 
 // One warp: the levels of spans 2..32 of the 32-leaf group at o (cnt <= 32 leaves), in registers.  Lane i
-// holds element i of the group; per level, every element's parent positions come from counting the smaller
-// elements of the sibling child (shuffles), the children's products are mapped to parent coordinates through
-// the group's slice of xs / ys, c*(r) of each row comes straight from its definition (delta(r, 0) by a ballot,
-// then one pass over the node's columns), and the lists are reordered through the group's slice of PL / QL.
-// Only __syncwarp: nothing here is shared with other warps.
+// holds element i of the group; per level, every element's parent position is its rank in the sibling child
+// (a binary search over the sibling's sorted lanes by shuffles), the children's products are mapped to parent
+// coordinates through the group's slice of xs / ys, and c*(r) of each row comes from its definition: with
+// L(r) = #{lo points in rows >= r} = -delta(r, 0), c*(r) - 1 is the column of the L(r)-th column g of the node
+// whose point raises delta in row r (one ballot per row of the node: bit g = colind(g, r)); the lists are
+// reordered through the group's slice of PL / QL.  Only __syncwarp: nothing here is shared with other warps.
 __device__ __forceinline__ void warp_low_levels(SaShared &S, int o, int cnt, int lane) {
     int pl = lane < cnt ? S.PL[o + lane] : INT_MAX;
     int ql = lane < cnt ? S.QL[o + lane] : INT_MAX;
     int res = 0;
-    for (int h = 1; h < 32 && h < cnt; h <<= 1) {
+#pragma unroll
+    for (int h = 1; h < 32; h <<= 1) {
+        if (h >= cnt) break;
         const int s = 2 * h;
         const int a = lane & ~(s - 1);
         const int m = min(a + h, cnt), b = min(a + s, cnt);
         const bool two = lane < cnt && m < b;   // the lane's node has both children
         const bool lo = lane < m;
-        // parent positions in the row-id (PL) and column-id (QL) merges
-        const int sb = lo ? m : a, se = lo ? b : m;
+        // parent positions in the row-id (PL) and column-id (QL) merges: the number of sibling entries below
+        // the lane's own (entries are distinct), by binary lifting over the sibling's sorted lanes [sb, se)
+        const int sb = lo ? m : a, len = lo ? b - m : m - a;
         int cp = 0, cq = 0;
-        for (int t = 0; t < h; ++t) {
-            const int src = (sb + t) & 31;
-            const int vp = __shfl_sync(kFull, pl, src);
-            const int vq = __shfl_sync(kFull, ql, src);
-            if (sb + t < se) {
-                cp += vp < pl;
-                cq += vq < ql;
-            }
+#pragma unroll
+        for (int step = h; step >= 1; step >>= 1) {
+            const int vp = __shfl_sync(kFull, pl, (sb + cp + step - 1) & 31);
+            const int vq = __shfl_sync(kFull, ql, (sb + cq + step - 1) & 31);
+            if (cp + step <= len && vp < pl) cp += step;
+            if (cq + step <= len && vq < ql) cq += step;
         }
         const int base = lo ? lane - a : lane - m;
         const int pp = two ? base + cp : lane - a;
@@ -295,16 +325,17 @@ __device__ __forceinline__ void warp_low_levels(SaShared &S, int o, int cnt, int
         const int k = b - a, r = lane - a;
         const unsigned lomask = __ballot_sync(kFull, two && !(x >> 15));
         const unsigned upto = b >= 32 ? 0xffffffffu : ((1u << b) - 1u);
-        int delta = -__popc(lomask & upto & ~((1u << lane) - 1u));
-        int cstar = delta >= 0 ? 0 : k + 1;
-        for (int c = 0; c < s; ++c) {
-            const int yc = __shfl_sync(kFull, y, (a + c) & 31);
-            if (c < k && cstar > k) {
-                const int yr = yc & 0x7fff;
-                delta += (yc >> 15) ? (yr < r) : (yr >= r);
-                if (delta >= 0) cstar = c + 1;
-            }
+        const int need = __popc(lomask & upto & ~((1u << lane) - 1u));
+        const int yr = y & 0x7fff;
+        const bool yhi = y >> 15;
+        unsigned mine = 0u;   // bit g: colind(g, r) for the columns g of the lane's node, row r = lane - a
+#pragma unroll
+        for (int i = 0; i < s; ++i) {
+            const unsigned M = __ballot_sync(kFull, two && (yhi ? (yr < i) : (yr >= i)));
+            if (r == i) mine = M;
         }
+        mine = (mine >> a) & (k >= 32 ? 0xffffffffu : ((1u << k) - 1u));
+        const int cstar = need == 0 ? 0 : (__popc(mine) >= need ? (int) __fns(mine, 0, need) + 1 : k + 1);
         if (two) {
             const int xr = x & 0x7fff;
             const bool hi = x >> 15;
@@ -427,18 +458,13 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
         // ---- ant passage for every node of this level that has two children ----
         const int nfull = nb / span;                  // nodes of size span
         const int rem = nb - nfull * span;            // size of the trailing node
-        const int nnodes = nfull + (rem > size ? 1 : 0);
         if (span > kSaSF) {
             // phase A: coarse boundaries (multiples of kSaSC inside each node).  c*(R) is the need-th column
             // raising delta in row R, need = the lo rows at or below R: counted once per kSaSC-row sub-band (warp
             // w: block rows [w kSaSC, (w+1) kSaSC), inside one node) and summed per boundary.
             if (warp * kSaSC < nb) {
                 const int r0 = warp * kSaSC, r1 = min(r0 + kSaSC, nb);
-                int cnt = 0;
-                for (int r = r0; r < r1; r += 32) {
-                    const int rr = r + lane;
-                    cnt += __popc(__ballot_sync(kFull, rr < r1 && !(S.xs[rr] >> 15)));
-                }
+                const int cnt = ballot_count<4>(r0, r1, lane, [&](int r) { return !(S.xs[r] >> 15); });
                 if (lane == 0) S.sub[warp] = cnt;
             }
             __syncthreads();
@@ -451,7 +477,7 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
                 const int R = (jj + 1) * kSaSC;
                 int need = 0;   // lo rows at or below R
                 for (int w = (a + R) / kSaSC; w * kSaSC < a + k; ++w) need += S.sub[w];
-                const int cst = warp_col_search(S, a, k, 0, need, R, lane);
+                const int cst = warp_col_search<4>(S, a, k, 0, need, R, lane);
                 if (lane == 0) S.cst[(a + R) / kSaSF] = cst;
             }
             __syncthreads();
@@ -479,61 +505,241 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
                 }
             }
             __syncthreads();
-            // phase C: walks of kSaSF rows, each from the c* of its bottom boundary.  The first warps walk one
-            // row band per thread; walks with a long column span are left to the remaining warps, which take
-            // them one whole warp each at the same time
-            const int wb_full = span / kSaSF;
-            const int wb_last = rem > size ? (rem + kSaSF - 1) / kSaSF : 0;
-            const int W = nfull * wb_full + wb_last;
-            const int nww = (W + 31) >> 5;
-            auto walk_of = [&](int t, int &a, int &k, int &top, int &bot) {
-                int nd, jj;
-                task_node(t, wb_full, nfull, nd, jj);
-                a = nd * span;
-                k = nd < nfull ? span : rem;
-                top = jj * kSaSF;
-                bot = min(top + kSaSF, k);
-            };
-            auto is_long = [&](int a, int k, int top, int bot) {
-                const int c = bot >= k ? 0 : S.cst[(a + bot) / kSaSF];
-                const int ce = S.cst[(a + top) / kSaSF];
-                return min(ce, k) - min(c, k) > kWalkSpanMax;
-            };
-            if (warp < nww) {
-                if (tid < W) {
-                    int a, k, top, bot;
-                    walk_of(tid, a, k, top, bot);
-                    if (!is_long(a, k, top, bot))
-                        thread_walk32(S, a, k, top, bot, bot >= k ? 0 : S.cst[(a + bot) / kSaSF]);
+            if (span < kSaRankSpan) {
+                // phase C: walks of kSaSF rows, each from the c* of its bottom boundary.  The first warps walk one
+                // row band per thread; walks with a long column span are left to the remaining warps, which take
+                // them one whole warp each at the same time
+                const int wb_full = span / kSaSF;
+                const int wb_last = rem > size ? (rem + kSaSF - 1) / kSaSF : 0;
+                const int W = nfull * wb_full + wb_last;
+                const int nww = (W + 31) >> 5;
+                auto walk_of = [&](int t, int &a, int &k, int &top, int &bot) {
+                    int nd, jj;
+                    task_node(t, wb_full, nfull, nd, jj);
+                    a = nd * span;
+                    k = nd < nfull ? span : rem;
+                    top = jj * kSaSF;
+                    bot = min(top + kSaSF, k);
+                };
+                auto is_long = [&](int a, int k, int top, int bot) {
+                    const int c = bot >= k ? 0 : S.cst[(a + bot) / kSaSF];
+                    const int ce = S.cst[(a + top) / kSaSF];
+                    return min(ce, k) - min(c, k) > kWalkSpanMax;
+                };
+                if (warp < nww) {
+                    if (tid < W) {
+                        int a, k, top, bot;
+                        walk_of(tid, a, k, top, bot);
+                        if (!is_long(a, k, top, bot))
+                            thread_walk32(S, a, k, top, bot, bot >= k ? 0 : S.cst[(a + bot) / kSaSF]);
+                    }
+                } else {
+                    const int h = warp - nww, nh = nwarps - nww;
+                    int seen = 0;
+                    for (int t0 = 0; t0 < W; t0 += 32) {
+                        bool lng = false;
+                        if (t0 + lane < W) {
+                            int a, k, top, bot;
+                            walk_of(t0 + lane, a, k, top, bot);
+                            lng = is_long(a, k, top, bot);
+                        }
+                        unsigned msk = __ballot_sync(kFull, lng);
+                        while (msk) {
+                            const int l = __ffs(msk) - 1;
+                            msk &= msk - 1;
+                            if (seen % nh == h) {
+                                int a, k, top, bot;
+                                walk_of(t0 + l, a, k, top, bot);
+                                warp_walk(S, a, k, top, bot, bot >= k ? 0 : S.cst[(a + bot) / kSaSF], lane);
+                            }
+                            ++seen;
+                        }
+                    }
                 }
             } else {
-                const int h = warp - nww, nh = nwarps - nww;
-                int seen = 0;
-                for (int t0 = 0; t0 < W; t0 += 32) {
-                    bool lng = false;
-                    if (t0 + lane < W) {
-                        int a, k, top, bot;
-                        walk_of(t0 + lane, a, k, top, bot);
-                        lng = is_long(a, k, top, bot);
+            // phase C: the rows whose point moves.  c*(r) is non-increasing in r and the product is a permutation,
+            // so the moving rows of a node take exactly their own columns, the topmost row the largest: a row moves
+            // iff delta(r, x_r) puts its point on the wrong side of c*(r) (hi: delta < 0, lo: delta >= 0), and the
+            // j-th moving row from the top takes the j-th largest of the moving rows' columns.  In the 32-row
+            // segment [R, bot) of row r, with cb = c*(bot) (where delta(bot, cb) = 0),
+            //   delta(r, x) = #{g in [cb, x): colind(g, bot)} - #{r' in [r, bot): rowind(r', x)},
+            // and a row with x < cb (delta < 0) or x >= c*(R) (delta >= 0) needs no count at all.
+            uint32_t *gbits = reinterpret_cast<uint32_t *>(S.posQ);   // moving rows, one bit per row
+            uint32_t *cbits = gbits + kSaSB / 32;                     // moving columns, one bit per column
+            int32_t *gpre = reinterpret_cast<int32_t *>(cbits + kSaSB / 32);   // exclusive prefixes of the words
+            int32_t *cpre = gpre + kSaSB / 32 + 1;
+            uint16_t *byrank = S.posP;                                // moving columns by descending rank
+            const int cov = nfull * span + (rem > size ? rem : 0);   // rows of the nodes with two children
+            const int nseg = (cov + 31) >> 5;
+            // Segments sg = warp + i nwarps, kSegB at a time: every load of a batch is issued before its results
+            // are used, and a segment's words are loaded by lane i and broadcast by shuffles.  Segment sg covers
+            // block rows [32 sg, 32 sg + 32), so its top's c* is cst[sg] and its bottom's cst[sg + 1] (0 at the
+            // bottom of the node).
+            for (int b0 = 0; b0 < kSegW; b0 += kSegB) {
+                int vv[kSegB];
+#pragma unroll
+                for (int i = 0; i < kSegB; ++i) {
+                    const int row = ((warp + (b0 + i) * nwarps) << 5) + lane;
+                    vv[i] = row < cov ? S.xs[row] : 0;
+                }
+                int ce_l = 0, cb_l = 0;
+                {
+                    const int sg = warp + (b0 + (lane & (kSegB - 1))) * nwarps;
+                    if (sg < nseg) {
+                        const int a = (sg << 5) & ~(span - 1);
+                        const int k = a < nfull * span ? span : rem;
+                        ce_l = S.cst[sg];
+                        cb_l = (sg << 5) - a + 32 >= k ? 0 : S.cst[sg + 1];
                     }
-                    unsigned msk = __ballot_sync(kFull, lng);
-                    while (msk) {
-                        const int l = __ffs(msk) - 1;
-                        msk &= msk - 1;
-                        if (seen % nh == h) {
-                            int a, k, top, bot;
-                            walk_of(t0 + l, a, k, top, bot);
-                            warp_walk(S, a, k, top, bot, bot >= k ? 0 : S.cst[(a + bot) / kSaSF], lane);
+                }
+#pragma unroll
+                for (int i = 0; i < kSegB; ++i) {
+                    const int sg = warp + (b0 + i) * nwarps;
+                    if (sg >= nseg) break;
+                    const int a = (sg << 5) & ~(span - 1);
+                    const int k = a < nfull * span ? span : rem;
+                    const int R = (sg << 5) - a, bot = min(R + 32, k);
+                    const int ce = __shfl_sync(kFull, ce_l, i), cb = __shfl_sync(kFull, cb_l, i);
+                    const bool valid = R + lane < k;
+                    const int v = vv[i];
+                    const int x = v & 0x7fff;
+                    const bool hi = v >> 15;
+                    bool good = x < cb ? hi : !hi;
+                    const bool hard = valid && x >= cb && x < ce;
+                    const unsigned hm = __ballot_sync(kFull, hard);
+                    if (hm) {
+                        int t2 = 0;   // rows [r, bot) whose point raises delta when moving up past them at column x
+                        for (unsigned rest = hm; rest; rest &= rest - 1) {
+                            const int hl = __ffs(rest) - 1;
+                            const int xh = __shfl_sync(kFull, x, hl);
+                            const unsigned mk =
+                                __ballot_sync(kFull, lane >= hl && R + lane < bot && (hi ? (x < xh) : (x >= xh)));
+                            if (lane == hl) t2 = __popc(mk);
                         }
-                        ++seen;
+                        const int xmax = (int) __reduce_max_sync(kFull, hard ? (unsigned) x : 0u);
+                        int t1 = 0;   // columns [cb, x) whose point raises delta in row bot
+                        for (int g0 = cb; g0 < xmax; g0 += 32) {
+                            const int g = g0 + lane;
+                            bool q = false;
+                            if (g < xmax) {
+                                const int w = S.ys[a + g];
+                                const int y = w & 0x7fff;
+                                q = (w >> 15) ? (y < bot) : (y >= bot);
+                            }
+                            const unsigned mk = __ballot_sync(kFull, q);
+                            if (x >= g0 + 32) t1 += __popc(mk);
+                            else if (x > g0) t1 += __popc(mk & ((1u << (x - g0)) - 1u));
+                        }
+                        if (hard) good = hi ? (t1 - t2 < 0) : (t1 - t2 >= 0);
+                    }
+                    const unsigned gm = __ballot_sync(kFull, valid && good);
+                    if (lane == 0) gbits[sg] = gm;
+                    if (valid && !good) S.RES[(sg << 5) + lane] = (uint16_t) x;   // a point that stays
+                }
+            }
+            __syncthreads();
+            // a column moves with the row that owns it
+            for (int b0 = 0; b0 < kSegW; b0 += kSegB) {
+                int yy[kSegB];
+#pragma unroll
+                for (int i = 0; i < kSegB; ++i) {
+                    const int col = ((warp + (b0 + i) * nwarps) << 5) + lane;
+                    yy[i] = col < cov ? (col & ~(span - 1)) + (S.ys[col] & 0x7fff) : -1;
+                }
+                uint32_t gw[kSegB];
+#pragma unroll
+                for (int i = 0; i < kSegB; ++i) gw[i] = yy[i] >= 0 ? gbits[yy[i] >> 5] >> (yy[i] & 31) : 0u;
+#pragma unroll
+                for (int i = 0; i < kSegB; ++i) {
+                    const int sg = warp + (b0 + i) * nwarps;
+                    const unsigned m = __ballot_sync(kFull, gw[i] & 1u);
+                    if (lane == 0 && sg < nseg) cbits[sg] = m;
+                }
+            }
+            __syncthreads();
+            if (warp < 2) {   // exclusive prefix counts of the row words (warp 0) and column words (warp 1)
+                const uint32_t *bits = warp == 0 ? gbits : cbits;
+                int32_t *pre = warp == 0 ? gpre : cpre;
+                int loc[kSaSB / 1024];
+                int sum = 0;
+#pragma unroll
+                for (int i = 0; i < kSaSB / 1024; ++i) {
+                    const int w = lane * (kSaSB / 1024) + i;
+                    loc[i] = w < nseg ? __popc(bits[w]) : 0;
+                    sum += loc[i];
+                }
+                int inc = sum;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int t = __shfl_up_sync(kFull, inc, d);
+                    if (lane >= d) inc += t;
+                }
+                int run = inc - sum;
+#pragma unroll
+                for (int i = 0; i < kSaSB / 1024; ++i) {
+                    const int w = lane * (kSaSB / 1024) + i;
+                    if (w < nseg) pre[w] = run;
+                    run += loc[i];
+                }
+                if (lane == 31) pre[nseg] = inc;
+            }
+            __syncthreads();
+            // moving columns by descending rank within the node
+            for (int b0 = 0; b0 < kSegW; b0 += kSegB) {
+                uint32_t cw_l = 0;
+                int p_l = 0, ps_l = 0, pe_l = 0;
+                {
+                    const int sg = warp + (b0 + (lane & (kSegB - 1))) * nwarps;
+                    if (sg < nseg) {
+                        const int a = (sg << 5) & ~(span - 1);
+                        const int k = a < nfull * span ? span : rem;
+                        cw_l = cbits[sg];
+                        p_l = cpre[sg];
+                        ps_l = cpre[a >> 5];
+                        pe_l = cpre[(a + k + 31) >> 5];
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < kSegB; ++i) {
+                    const int sg = warp + (b0 + i) * nwarps;
+                    if (sg >= nseg) break;
+                    const uint32_t cw = __shfl_sync(kFull, cw_l, i);
+                    const int p = __shfl_sync(kFull, p_l, i), ps = __shfl_sync(kFull, ps_l, i),
+                              pe = __shfl_sync(kFull, pe_l, i);
+                    if ((cw >> lane) & 1u) {
+                        const int col = (sg << 5) + lane, a = col & ~(span - 1);
+                        const int incl = p - ps + __popc(cw & ((2u << lane) - 1u));
+                        byrank[a + (pe - ps) - incl] = (uint16_t) (col - a);
                     }
                 }
             }
-        } else {
-            for (int node = tid; node < nnodes; node += kSaThreads) {
-                const int a = node * span;
-                const int k = node < nfull ? span : rem;
-                thread_walk(S, a, k, 0, k, 0);
+            __syncthreads();
+            // the moving rows, the j-th from the top of its node taking the j-th largest moving column
+            for (int b0 = 0; b0 < kSegW; b0 += kSegB) {
+                uint32_t gw_l = 0;
+                int p_l = 0, ps_l = 0;
+                {
+                    const int sg = warp + (b0 + (lane & (kSegB - 1))) * nwarps;
+                    if (sg < nseg) {
+                        gw_l = gbits[sg];
+                        p_l = gpre[sg];
+                        ps_l = gpre[((sg << 5) & ~(span - 1)) >> 5];
+                    }
+                }
+                uint16_t val[kSegB];
+#pragma unroll
+                for (int i = 0; i < kSegB; ++i) {
+                    const uint32_t gw = __shfl_sync(kFull, gw_l, i);
+                    const int p = __shfl_sync(kFull, p_l, i), ps = __shfl_sync(kFull, ps_l, i);
+                    const int a = ((warp + (b0 + i) * nwarps) << 5) & ~(span - 1);
+                    val[i] = ((gw >> lane) & 1u) ? byrank[a + p - ps + __popc(gw & ((1u << lane) - 1u))] : 0;
+                }
+#pragma unroll
+                for (int i = 0; i < kSegB; ++i) {
+                    const uint32_t gw = __shfl_sync(kFull, gw_l, i);
+                    if ((gw >> lane) & 1u) S.RES[((warp + (b0 + i) * nwarps) << 5) + lane] = val[i];
+                }
+            }
             }
         }
         __syncthreads();
@@ -555,16 +761,20 @@ constexpr int kBandSub = kBand / (kBandThreads / 32);   // rows per warp sub-ban
 constexpr int kBandWalk = kBand / kBandThreads;         // rows per thread walk
 constexpr int kBandYCap = 12288;   // columns a band stages in shared memory
 constexpr unsigned kHiBit = 1u << 30;
+constexpr int kRowHistSmemMax = 200 * 1024;   // block-table width limit of sa_rowhist_kernel's histogram
 constexpr int kValMask = (1 << 30) - 1;
 
 struct SaNode {
     int64_t off;       // first common index of the node
     int k;             // node size
     int h;             // size of the lo child (k - h = hi child)
-    int Sc;            // rows/cols per table block (a power of two; divides kBand when Sc <= kBand)
-    int G;             // table blocks per dimension: ceil(k / Sc)
-    int64_t tab_off;   // offset of the node's (G+1) x (G+1) prefix table
-    int64_t vec_off;   // offset of the node's lo-row / lo-col counts (G+1 each)
+    int Sc;            // columns per table column block (a power of two)
+    int G;             // table column blocks: ceil(k / Sc)
+    int Sr;            // rows per table row block: max(Sc, kBand), so every band boundary that is a multiple of Sr
+                       // is a table row
+    int NR;            // table row blocks: ceil(k / Sr)
+    int64_t tab_off;   // offset of the node's (NR+1) x (G+1) prefix table
+    int64_t vec_off;   // offset of the node's lo-row prefix (NR+1 entries) and lo-col prefix (G+1 entries)
     int64_t cst_off;   // offset of the node's c* slots, one per band (row b kBand)
 };
 
@@ -573,34 +783,43 @@ struct SaTile {
     int t;      // tile index inside the node
 };
 
-__device__ __forceinline__ int merge_path(const int32_t *lo, int nlo, const int32_t *hi, int nhi, int diag) {
-    int l = max(0, diag - nhi), h = min(diag, nlo);
-    while (l < h) {
-        const int mid = (l + h) >> 1;
-        if (lo[mid] < hi[diag - 1 - mid]) l = mid + 1;
-        else h = mid;
-    }
-    return l;
+// Merge-path splits of every merge tile's first output, of the row-id lists (.x) and the column-id lists (.y):
+// one warp per tile and list (33-way search), so no merge CTA starts with a serial search of global memory.
+__global__ void __launch_bounds__(256) sa_split_kernel(const SaNode *__restrict__ nodes, const SaTile *__restrict__ tiles,
+                                                       int ntiles, const int32_t *__restrict__ PL,
+                                                       const int32_t *__restrict__ QL, int2 *__restrict__ splits) {
+    const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (w >= 2 * ntiles) return;
+    const int t = w >> 1, which = w & 1;
+    const SaTile tl = tiles[t];
+    const SaNode nd = nodes[tl.node];
+    const int nhi = nd.k - nd.h, o0 = tl.t * kMT;
+    const int32_t *lo = (which ? QL : PL) + nd.off, *hi = lo + nd.h;
+    // the merge path's split at diagonal o0: the first i with lo[i] >= hi[o0 - 1 - i]
+    const int i = warp_first_true(max(0, o0 - nhi), min(o0, nd.h), lane,
+                                  [&](int m) { return __ldg(lo + m) >= __ldg(hi + o0 - 1 - m); });
+    if (lane == 0) reinterpret_cast<int *>(splits)[2 * t + which] = i;
 }
 
 // Merge the children's sorted lists of every node; pos receives the node-local parent position of every
-// child element (the reference's row / column mappers).
+// child element (the reference's row / column mappers).  which = 0: row-id lists (splits .x), 1: column-id lists.
 __global__ void __launch_bounds__(256) sa_merge_kernel(const SaNode *__restrict__ nodes, const SaTile *__restrict__ tiles,
+                                                       const int2 *__restrict__ splits, int which,
                                                        const int32_t *__restrict__ Lin, int32_t *__restrict__ Lout,
                                                        int32_t *__restrict__ pos) {
     __shared__ int32_t sm_lo[kMT], sm_hi[kMT];
-    __shared__ int split[2];
     const SaTile tl = tiles[blockIdx.x];
     const SaNode nd = nodes[tl.node];
-    const int32_t *lo = Lin + nd.off, *hi = Lin + nd.off + nd.h;
-    const int nlo = nd.h, nhi = nd.k - nd.h;
+    const int nlo = nd.h;
     const int o0 = tl.t * kMT, o1 = min(o0 + kMT, nd.k);
-    if (threadIdx.x == 0) {
-        split[0] = merge_path(lo, nlo, hi, nhi, o0);
-        split[1] = merge_path(lo, nlo, hi, nhi, o1);
+    const int2 s0 = splits[blockIdx.x];
+    int i1 = nlo;   // the node's last tile ends with both lists consumed
+    if (o1 < nd.k) {
+        const int2 s1 = splits[blockIdx.x + 1];   // the next tile of the same node
+        i1 = which ? s1.y : s1.x;
     }
-    __syncthreads();
-    const int i0 = split[0], i1 = split[1], j0 = o0 - i0, j1 = o1 - i1;
+    const int32_t *lo = Lin + nd.off, *hi = Lin + nd.off + nd.h;
+    const int i0 = which ? s0.y : s0.x, j0 = o0 - i0, j1 = o1 - i1;
     const int na = i1 - i0, nbb = j1 - j0;
     for (int x = threadIdx.x; x < na; x += blockDim.x) sm_lo[x] = lo[i0 + x];
     for (int x = threadIdx.x; x < nbb; x += blockDim.x) sm_hi[x] = hi[j0 + x];
@@ -619,12 +838,11 @@ __global__ void __launch_bounds__(256) sa_merge_kernel(const SaNode *__restrict_
     }
 }
 
-// Children's products in the parent's coordinates, signed block counts (hi +1, lo -1), lo-row / lo-col counts.
+// Children's products in the parent's coordinates: xs (row -> col | hi) and ys (col -> row | hi).
 __global__ void __launch_bounds__(256) sa_map_kernel(const SaNode *__restrict__ nodes, const SaTile *__restrict__ tiles,
                                                      const int32_t *__restrict__ posP, const int32_t *__restrict__ posQ,
                                                      const int32_t *__restrict__ RES, int32_t *__restrict__ xs,
-                                                     int32_t *__restrict__ ys, int32_t *__restrict__ tab,
-                                                     int32_t *__restrict__ vec, int *err) {
+                                                     int32_t *__restrict__ ys, int *err) {
     const SaTile tl = tiles[blockIdx.x];
     const SaNode nd = nodes[tl.node];
     const int e0 = tl.t * kMT, e1 = min(e0 + kMT, nd.k);
@@ -640,39 +858,56 @@ __global__ void __launch_bounds__(256) sa_map_kernel(const SaNode *__restrict__ 
         const int col = posQ[nd.off + cs + rc];
         xs[nd.off + row] = col | (hi ? kHiBit : 0);
         ys[nd.off + col] = row | (hi ? kHiBit : 0);
-        const int g = row / nd.Sc, hh = col / nd.Sc;
-        atomicAdd(&tab[nd.tab_off + (int64_t) g * (nd.G + 1) + hh], hi ? 1 : -1);
-        if (!hi) {
-            atomicAdd(&vec[nd.vec_off + g], 1);                  // lo rows per row block
-            atomicAdd(&vec[nd.vec_off + (nd.G + 1) + hh], 1);    // lo cols per col block
-        }
     }
 }
 
-// Exclusive prefix sums of the block counts: along h for every row g (dir 0), then along g for every
-// column h (dir 1); the two lo-count vectors are scanned by the dir-0 lines G+1 and G+2.
-__global__ void __launch_bounds__(256) sa_scan_kernel(const SaNode *__restrict__ nodes, const int2 *__restrict__ lines,
-                                                      int32_t *__restrict__ tab, int32_t *__restrict__ vec, int dir) {
-    const int2 ln = lines[blockIdx.x];   // (node, line index)
-    const SaNode nd = nodes[ln.x];
-    const int W = nd.G + 1;
-    int32_t *base;
-    int64_t stride;
-    if (ln.y < W) {
-        base = tab + nd.tab_off + (dir == 0 ? (int64_t) ln.y * W : ln.y);
-        stride = dir == 0 ? 1 : W;
-    } else {
-        base = vec + nd.vec_off + (int64_t) (ln.y - W) * W;
-        stride = 1;
+// number of entries < v in the increasing sequence a[0, n)
+__device__ __forceinline__ int lower_bound_g(const int32_t *__restrict__ a, int n, int v) {
+    int l = 0, h = n;
+    while (l < h) {
+        const int mid = (l + h) >> 1;
+        if (__ldg(a + mid) < v) l = mid + 1;
+        else h = mid;
     }
+    return l;
+}
+
+// Row g of a node's block table (one CTA per row block of Sr rows, g = 0..NR): the signed counts of the row
+// block's points by column block (hi +1, lo -1) in a shared histogram, scanned along the columns (exclusive)
+// into the table; row NR is all zeros (the column scan's total row).  The lo-row prefix (entry g) and the lo-col
+// prefix (entries h = g mod (NR+1)) come from binary searches: the lo child's rows and columns in the parent
+// are its merge positions, two increasing sequences, so the lo rows (columns) before a bound are a search.
+__global__ void __launch_bounds__(256) sa_rowhist_kernel(const SaNode *__restrict__ nodes, const int2 *__restrict__ tasks,
+                                                         const int32_t *__restrict__ xs, const int32_t *__restrict__ posP,
+                                                         const int32_t *__restrict__ posQ, int32_t *__restrict__ tab,
+                                                         int32_t *__restrict__ vec) {
+    extern __shared__ int32_t hist[];   // G + 1 counters
     __shared__ int32_t warp_sums[8];
     __shared__ int32_t carry;
+    const int2 tk = tasks[blockIdx.x];   // (node, row block)
+    const SaNode nd = nodes[tk.x];
+    const int W = nd.G + 1, g = tk.y;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int h = threadIdx.x; h < W; h += blockDim.x) hist[h] = 0;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == blockDim.x - 1)
+        vec[nd.vec_off + g] = lower_bound_g(posP + nd.off, nd.h, (int) min((int64_t) g * nd.Sr, (int64_t) INT_MAX));
+    for (int h = g + (int) threadIdx.x * (nd.NR + 1); h < W; h += (int) blockDim.x * (nd.NR + 1))
+        vec[nd.vec_off + nd.NR + 1 + h] = lower_bound_g(posQ + nd.off, nd.h, (int) min((int64_t) h * nd.Sc, (int64_t) INT_MAX));
+    if (g < nd.NR) {
+        const int r0 = g * nd.Sr, r1 = min(r0 + nd.Sr, nd.k);
+        for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+            const int v = xs[nd.off + r];
+            const int hh = (v & kValMask) / nd.Sc;
+            if (hh < W) atomicAdd(&hist[hh], (v & kHiBit) ? 1 : -1);
+        }
+    }
+    __syncthreads();
+    int32_t *row = tab + nd.tab_off + (int64_t) g * W;
     for (int c0 = 0; c0 < W; c0 += blockDim.x) {
         const int c = c0 + threadIdx.x;
-        const int v = c < W ? base[c * stride] : 0;
+        const int v = c < W ? hist[c] : 0;
         int incl = v;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -685,27 +920,31 @@ __global__ void __launch_bounds__(256) sa_scan_kernel(const SaNode *__restrict__
         for (int w = 0; w < warp; ++w) woff += warp_sums[w];
         const int excl = carry + woff + incl - v;
         __syncthreads();
-        if (c < W) base[c * stride] = excl;
+        if (c < W) row[c] = excl;
         if (threadIdx.x == blockDim.x - 1) carry = excl + v;
         __syncthreads();
     }
 }
 
-// Exclusive prefix sums along g of 32 table columns per block (lanes = columns, so every row access is one
-// coalesced segment); the 8 warps take 8 consecutive row ranges and combine their column totals.
-__global__ void __launch_bounds__(256) sa_scan_cols_kernel(const SaNode *__restrict__ nodes,
-                                                           const int2 *__restrict__ groups, int32_t *__restrict__ tab) {
+// Exclusive prefix sums along g (the NR+1 table rows) of 32 table columns per block (lanes = columns, so every
+// row access is one coalesced segment); the kScanColWarps warps take consecutive row ranges and combine their
+// column totals.
+constexpr int kScanColWarps = 32;
+__global__ void __launch_bounds__(kScanColWarps * 32) sa_scan_cols_kernel(const SaNode *__restrict__ nodes,
+                                                                          const int2 *__restrict__ groups,
+                                                                          int32_t *__restrict__ tab) {
     const int2 gr = groups[blockIdx.x];   // (node, first column)
     const SaNode nd = nodes[gr.x];
-    const int W = nd.G + 1;
+    const int W = nd.G + 1, NG = nd.NR + 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int h = gr.y + lane;
     const bool act = h < W;
     int32_t *col = tab + nd.tab_off + h;   // entry (g, h) at col[g W]
-    const int per = (W + 7) / 8, g0 = min(W, warp * per), g1 = min(W, g0 + per);
-    __shared__ int32_t part[8][32];
+    const int per = (NG + kScanColWarps - 1) / kScanColWarps, g0 = min(NG, warp * per), g1 = min(NG, g0 + per);
+    __shared__ int32_t part[kScanColWarps][32];
     int sum = 0;
     if (act)
+#pragma unroll 4
         for (int g = g0; g < g1; ++g) sum += col[(int64_t) g * W];
     part[warp][lane] = sum;
     __syncthreads();
@@ -720,43 +959,28 @@ __global__ void __launch_bounds__(256) sa_scan_cols_kernel(const SaNode *__restr
 }
 
 __device__ __forceinline__ int hbm_delta_corner(const SaNode &nd, const int32_t *tab, const int32_t *vec, int g, int h) {
-    // delta(g Sc, h Sc) = #{hi: row < g Sc, col < h Sc} - #{lo: row < g Sc, col < h Sc}
-    //                    + #{lo: row < g Sc} + #{lo: col < h Sc} - #lo       (tab holds the signed prefix)
+    // delta(g Sr, h Sc) = #{hi: row < g Sr, col < h Sc} - #{lo: row < g Sr, col < h Sc}
+    //                    + #{lo: row < g Sr} + #{lo: col < h Sc} - #lo       (tab holds the signed prefix)
     const int W = nd.G + 1;
-    return tab[nd.tab_off + (int64_t) g * W + h] + vec[nd.vec_off + g] + vec[nd.vec_off + W + h] - nd.h;
+    return tab[nd.tab_off + (int64_t) g * W + h] + vec[nd.vec_off + g] + vec[nd.vec_off + nd.NR + 1 + h] - nd.h;
 }
 
+template <int U = 1>
 __device__ __forceinline__ int hbm_row_count(const int32_t *xs, int64_t off, int r0, int r1, int c, int lane) {
-    int total = 0;
-    for (int r = r0; r < r1; r += 32) {
-        const int rr = r + lane;
-        bool q = false;
-        if (rr < r1) {
-            const int v = xs[off + rr];
-            const int x = v & kValMask;
-            q = (v & kHiBit) ? (x < c) : (x >= c);
-        }
-        total += __popc(__ballot_sync(kFull, q));
-    }
-    return total;
+    return ballot_count<U>(r0, r1, lane, [&](int r) {
+        const int v = xs[off + r];
+        const int x = v & kValMask;
+        return (v & kHiBit) ? (x < c) : (x >= c);
+    });
 }
 
+template <int U = 1>
 __device__ __forceinline__ int hbm_col_search(const int32_t *ys, int64_t off, int k, int from, int need, int R, int lane) {
-    if (need <= 0) return from;
-    for (int g0 = from; g0 < k; g0 += 32) {
-        const int g = g0 + lane;
-        bool q = false;
-        if (g < k) {
-            const int w = ys[off + g];
-            const int y = w & kValMask;
-            q = (w & kHiBit) ? (y < R) : (y >= R);
-        }
-        const unsigned mask = __ballot_sync(kFull, q);
-        const int cnt = __popc(mask);
-        if (need <= cnt) return g0 + (int) __fns(mask, 0, need) + 1;
-        need -= cnt;
-    }
-    return k + 1;
+    return ballot_search<U>(from, k, need, k + 1, lane, [&](int g) {
+        const int w = ys[off + g];
+        const int y = w & kValMask;
+        return (w & kHiBit) ? (y < R) : (y >= R);
+    });
 }
 
 // c* at the band boundaries R = b kBand that are multiples of Sc (one warp each): the table locates the
@@ -770,19 +994,15 @@ __global__ void __launch_bounds__(256) sa_coarse_kernel(const SaNode *__restrict
     if (t >= ntasks) return;
     const int2 tk = tasks[t];   // (node, band)
     const SaNode nd = nodes[tk.x];
-    const int R = tk.y * kBand, g = R / nd.Sc;
-    int l = 0, hgh = nd.G + 1;   // first h with delta(R, min(h Sc, k)) >= 0
-    while (l < hgh) {
-        const int mid = (l + hgh) >> 1;
-        if (hbm_delta_corner(nd, tab, vec, g, mid) >= 0) hgh = mid;
-        else l = mid + 1;
-    }
+    const int R = tk.y * kBand, g = R / nd.Sr;
+    // first h with delta(R, min(h Sc, k)) >= 0
+    const int l = warp_first_true(0, nd.G + 1, lane, [&](int h) { return hbm_delta_corner(nd, tab, vec, g, h) >= 0; });
     int c;
     if (l == 0) c = 0;
     else if (l > nd.G) c = nd.k + 1;
     else {
         const int need = -hbm_delta_corner(nd, tab, vec, g, l - 1);
-        c = hbm_col_search(ys, nd.off, nd.k, (l - 1) * nd.Sc, need, R, lane);
+        c = hbm_col_search<4>(ys, nd.off, nd.k, (l - 1) * nd.Sc, need, R, lane);
     }
     if (lane == 0) cst[nd.cst_off + tk.y] = c;
 }
@@ -798,12 +1018,12 @@ __global__ void __launch_bounds__(256) sa_fine_kernel(const SaNode *__restrict__
     const int2 tk = tasks[t];   // (node, band)
     const SaNode nd = nodes[tk.x];
     const int R = tk.y * kBand;
-    const int Rb = min((R / nd.Sc + 1) * nd.Sc, nd.k);
+    const int Rb = min((R / nd.Sr + 1) * nd.Sr, nd.k);
     const int cb = Rb >= nd.k ? 0 : cst[nd.cst_off + Rb / kBand];
     int c = nd.k + 1;
     if (cb <= nd.k) {
-        const int need = hbm_row_count(xs, nd.off, R, Rb, cb, lane);
-        c = hbm_col_search(ys, nd.off, nd.k, cb, need, R, lane);
+        const int need = hbm_row_count<4>(xs, nd.off, R, Rb, cb, lane);
+        c = hbm_col_search<4>(ys, nd.off, nd.k, cb, need, R, lane);
     }
     if (lane == 0) cst[nd.cst_off + tk.y] = c;
 }
@@ -829,38 +1049,23 @@ struct YView {
 };
 
 // warp-wide: rows i in [i0, i1) of the band whose point raises delta when moving up past it at column c
+template <int U = 1>
 __device__ __forceinline__ int band_row_count(const int32_t *X, int i0, int i1, int c, int lane) {
-    int total = 0;
-    for (int i = i0; i < i1; i += 32) {
-        const int ii = i + lane;
-        bool q = false;
-        if (ii < i1) {
-            const int v = X[ii];
-            const int x = v & kValMask;
-            q = (v & kHiBit) ? (x < c) : (x >= c);
-        }
-        total += __popc(__ballot_sync(kFull, q));
-    }
-    return total;
+    return ballot_count<U>(i0, i1, lane, [&](int i) {
+        const int v = X[i];
+        const int x = v & kValMask;
+        return (v & kHiBit) ? (x < c) : (x >= c);
+    });
 }
 
 // warp-wide: one past the need-th column g in [from, cend) whose point raises delta in row R; k + 1 if none
+template <int U = 1>
 __device__ __forceinline__ int band_col_search(const YView &Y, int k, int from, int cend, int need, int R, int lane) {
-    if (need <= 0) return from;
-    for (int g0 = from; g0 < cend; g0 += 32) {
-        const int g = g0 + lane;
-        bool q = false;
-        if (g < cend) {
-            const int w = Y(g);
-            const int y = w & kValMask;
-            q = (w & kHiBit) ? (y < R) : (y >= R);
-        }
-        const unsigned mask = __ballot_sync(kFull, q);
-        const int cnt = __popc(mask);
-        if (need <= cnt) return g0 + (int) __fns(mask, 0, need) + 1;
-        need -= cnt;
-    }
-    return k + 1;
+    return ballot_search<U>(from, cend, need, k + 1, lane, [&](int g) {
+        const int w = Y(g);
+        const int y = w & kValMask;
+        return (w & kHiBit) ? (y < R) : (y >= R);
+    });
 }
 
 // one thread: band rows [i0, i1) walked up from c = c*(R0 + i1)
@@ -955,7 +1160,7 @@ __global__ void __launch_bounds__(kBandThreads) sa_band_kernel(const SaNode *__r
     // that raise delta at cbot are counted once per sub-band (each warp its own), and summed over the warps below.
     if (cbot <= k && warp * kBandSub < nr) {
         const int i0 = warp * kBandSub, i1 = min(i0 + kBandSub, nr);
-        const int cnt = band_row_count(S.x, i0, i1, cbot, lane);
+        const int cnt = band_row_count<4>(S.x, i0, i1, cbot, lane);
         if (lane == 0) S.subcnt[warp] = cnt;
     }
     __syncthreads();
@@ -965,7 +1170,7 @@ __global__ void __launch_bounds__(kBandThreads) sa_band_kernel(const SaNode *__r
         if (cbot <= k) {
             int need = 0;
             for (int w = warp; w < nwarps && w * kBandSub < nr; ++w) need += S.subcnt[w];
-            c = band_col_search(Y, k, cbot, cend, need, R0 + i, lane);
+            c = band_col_search<4>(Y, k, cbot, cend, need, R0 + i, lane);
         }
         if (lane == 0) S.cst[warp * wsub] = c;
     }
@@ -1062,10 +1267,13 @@ struct SaPlan {
     SaTile *d_tiles = nullptr;
     int2 *d_tasks = nullptr;
     int64_t *d_copies = nullptr;
+    int2 *d_splits = nullptr;     // merge-path splits of the merge tiles of one level
+    int max_tiles = 0;
     int32_t *pinv = nullptr, *pl[2] = {nullptr, nullptr}, *ql[2] = {nullptr, nullptr}, *res[2] = {nullptr, nullptr};
     int32_t *posP = nullptr, *posQ = nullptr, *xs = nullptr, *ys = nullptr, *tab = nullptr, *vec = nullptr,
             *cst = nullptr;
     int64_t tab_max = 0, vec_max = 0, cst_max = 0;
+    int max_w = 0;                 // widest block table (G + 1) of any level
     cudaStream_t alloc_stream = nullptr;
     bool shared_scratch = false;   // per-element scratch owned by the caller
 };
@@ -1103,7 +1311,8 @@ int sa_plan_bind(SaPlan *P, const SaScratch *sh) {
 void sa_plan_destroy(SaPlan *P) {
     if (!P) return;
     cudaStream_t s = P->alloc_stream;
-    void *ptrs[] = {P->d_probs, P->d_probtiles, P->d_items, P->d_nodes, P->d_tiles, P->d_tasks, P->d_copies};
+    void *ptrs[] = {P->d_probs, P->d_probtiles, P->d_items, P->d_nodes, P->d_tiles, P->d_tasks, P->d_copies,
+                    P->d_splits};
     for (void *p : ptrs) dfree(p, s);
     if (!P->shared_scratch) {
         void *sp[] = {P->pinv, P->pl[0], P->pl[1], P->ql[0], P->ql[1], P->res[0], P->res[1], P->posP, P->posQ,
@@ -1175,9 +1384,10 @@ int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, S
                 while ((int64_t) Sc * Sc < k) Sc <<= 1;
                 while (Sc < kBand && k / Sc > 1024) Sc <<= 1;   // a (G+1)^2 table of at most ~1024^2 entries
                 const int G = (k + Sc - 1) / Sc;
-                nodes.push_back(SaNode{off[i] + a, k, h, Sc, G, L.tab_tot, L.vec_tot, L.cst_tot});
-                L.tab_tot += (int64_t) (G + 1) * (G + 1);
-                L.vec_tot += 2 * (int64_t) (G + 1);
+                const int Sr = std::max(Sc, kBand), NR = (k + Sr - 1) / Sr;
+                nodes.push_back(SaNode{off[i] + a, k, h, Sc, G, Sr, NR, L.tab_tot, L.vec_tot, L.cst_tot});
+                L.tab_tot += (int64_t) (NR + 1) * (G + 1);
+                L.vec_tot += (int64_t) (NR + 1) + (G + 1);
                 L.cst_tot += (k + kBand - 1) / kBand + 1;
             }
         }
@@ -1187,9 +1397,12 @@ int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, S
         for (int j = 0; j < L.nnodes; ++j)
             for (int t = 0; (int64_t) t * kMT < nodes[first_node + j].k; ++t) tiles.push_back(SaTile{j, t});
         L.ntiles = (int) (tiles.size() - L.o_tiles);
+        P->max_tiles = std::max(P->max_tiles, L.ntiles);
         L.o_l0 = (int64_t) tasks.size();
-        for (int j = 0; j < L.nnodes; ++j)
-            for (int y = 0; y < nodes[first_node + j].G + 3; ++y) tasks.push_back(make_int2(j, y));
+        for (int j = 0; j < L.nnodes; ++j) {
+            for (int y = 0; y < nodes[first_node + j].NR + 1; ++y) tasks.push_back(make_int2(j, y));
+            P->max_w = std::max(P->max_w, nodes[first_node + j].G + 1);
+        }
         L.nl0 = (int) (tasks.size() - L.o_l0);
         L.o_l1 = (int64_t) tasks.size();
         for (int j = 0; j < L.nnodes; ++j)
@@ -1200,20 +1413,22 @@ int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, S
         for (int j = 0; j < L.nnodes; ++j) {
             const SaNode &nd = nodes[first_node + j];
             for (int b = 0; (int64_t) b * kBand < nd.k; ++b)
-                if (((int64_t) b * kBand) % nd.Sc == 0) tasks.push_back(make_int2(j, b));
+                if (((int64_t) b * kBand) % nd.Sr == 0) tasks.push_back(make_int2(j, b));
         }
         L.nct = (int) (tasks.size() - L.o_ct);
         L.o_ft = (int64_t) tasks.size();
         for (int j = 0; j < L.nnodes; ++j) {
             const SaNode &nd = nodes[first_node + j];
             for (int b = 0; (int64_t) b * kBand < nd.k; ++b)
-                if (((int64_t) b * kBand) % nd.Sc != 0) tasks.push_back(make_int2(j, b));
+                if (((int64_t) b * kBand) % nd.Sr != 0) tasks.push_back(make_int2(j, b));
         }
         L.nft = (int) (tasks.size() - L.o_ft);
         L.o_wt = (int64_t) tasks.size();
         for (int j = 0; j < L.nnodes; ++j)
             for (int b = 0; (int64_t) b * kBand < nodes[first_node + j].k; ++b) tasks.push_back(make_int2(j, b));
         L.nwt = (int) (tasks.size() - L.o_wt);
+        if ((int64_t) P->max_w * (int64_t) sizeof(int32_t) > kRowHistSmemMax)
+            return bail(fail(SLCS_ERR_ARG, "steady ant: product too large for the block-table histogram"));
         P->tab_max = std::max(P->tab_max, L.tab_tot);
         P->vec_max = std::max(P->vec_max, L.vec_tot);
         P->cst_max = std::max(P->cst_max, L.cst_tot);
@@ -1223,7 +1438,8 @@ int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, S
     if ((rc = plan_upload(&P->d_probs, probs, s)) || (rc = plan_upload(&P->d_probtiles, probtiles, s)) ||
         (rc = plan_upload(&P->d_items, items, s)) || (rc = plan_upload(&P->d_nodes, nodes, s)) ||
         (rc = plan_upload(&P->d_tiles, tiles, s)) || (rc = plan_upload(&P->d_tasks, tasks, s)) ||
-        (rc = plan_upload(&P->d_copies, copies, s)))
+        (rc = plan_upload(&P->d_copies, copies, s)) ||
+        (rc = dalloc(reinterpret_cast<void **>(&P->d_splits), sizeof(int2) * std::max(P->max_tiles, 1), s)))
         return bail(rc);
     const int64_t T = std::max<int64_t>(P->total, 1);
     if (shared) {
@@ -1249,6 +1465,8 @@ int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, S
                                              (int) sizeof(SaShared));
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(sa_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(BandShared));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(sa_rowhist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowHistSmemMax);
         if (e != cudaSuccess) return bail(fail(SLCS_ERR_CUDA, "cudaFuncSetAttribute(steady-ant kernels) failed"));
         attr_set = true;
     }
@@ -1297,15 +1515,15 @@ int sa_plan_run_ex(SaPlan *P, const int32_t *d_P, const int32_t *d_leafP, const 
         const int nxt = cur ^ 1;
         const SaNode *nodes = P->d_nodes + L.o_nodes;
         if (L.nnodes) {
-            SLCS_CUDA_TRY(cudaMemsetAsync(P->tab, 0, sizeof(int32_t) * L.tab_tot, s));
-            SLCS_CUDA_TRY(cudaMemsetAsync(P->vec, 0, sizeof(int32_t) * L.vec_tot, s));
             const SaTile *tiles = P->d_tiles + L.o_tiles;
-            sa_merge_kernel<<<L.ntiles, 256, 0, s>>>(nodes, tiles, P->pl[cur], P->pl[nxt], P->posP);
-            sa_merge_kernel<<<L.ntiles, 256, 0, s>>>(nodes, tiles, P->ql[cur], P->ql[nxt], P->posQ);
-            sa_map_kernel<<<L.ntiles, 256, 0, s>>>(nodes, tiles, P->posP, P->posQ, P->res[cur], P->xs, P->ys, P->tab,
-                                                   P->vec, d_err);
-            sa_scan_kernel<<<L.nl0, 256, 0, s>>>(nodes, P->d_tasks + L.o_l0, P->tab, P->vec, 0);
-            sa_scan_cols_kernel<<<L.nl1, 256, 0, s>>>(nodes, P->d_tasks + L.o_l1, P->tab);
+            sa_split_kernel<<<(2 * L.ntiles + 7) / 8, 256, 0, s>>>(nodes, tiles, L.ntiles, P->pl[cur], P->ql[cur],
+                                                                  P->d_splits);
+            sa_merge_kernel<<<L.ntiles, 256, 0, s>>>(nodes, tiles, P->d_splits, 0, P->pl[cur], P->pl[nxt], P->posP);
+            sa_merge_kernel<<<L.ntiles, 256, 0, s>>>(nodes, tiles, P->d_splits, 1, P->ql[cur], P->ql[nxt], P->posQ);
+            sa_map_kernel<<<L.ntiles, 256, 0, s>>>(nodes, tiles, P->posP, P->posQ, P->res[cur], P->xs, P->ys, d_err);
+            sa_rowhist_kernel<<<L.nl0, 256, sizeof(int32_t) * P->max_w, s>>>(nodes, P->d_tasks + L.o_l0, P->xs, P->posP,
+                                                                             P->posQ, P->tab, P->vec);
+            sa_scan_cols_kernel<<<L.nl1, kScanColWarps * 32, 0, s>>>(nodes, P->d_tasks + L.o_l1, P->tab);
             if (L.nct)
                 sa_coarse_kernel<<<(L.nct + 7) / 8, 256, 0, s>>>(nodes, P->d_tasks + L.o_ct, L.nct, P->tab, P->vec,
                                                                  P->ys, P->cst);
@@ -1333,7 +1551,7 @@ int sa_plan_run(SaPlan *P, const int32_t *d_P, const int32_t *d_Q, int32_t *d_R,
 
 int sa_plan_launches(const SaPlan *P) {
     int c = (P->nprobtiles ? 1 : 0) + (P->nitems ? 1 : 0);
-    for (const SaLevel &L : P->levels) c += (L.nnodes ? 6 + (L.nct ? 1 : 0) + (L.nft ? 1 : 0) : 0) + (L.ncopies ? 1 : 0);
+    for (const SaLevel &L : P->levels) c += (L.nnodes ? 7 + (L.nct ? 1 : 0) + (L.nft ? 1 : 0) : 0) + (L.ncopies ? 1 : 0);
     return c;
 }
 
