@@ -40,6 +40,7 @@ constexpr int kSaRankSpan = 1024;  // node spans from which the moving rows are 
 constexpr int kSegW = kSaSB / 32 / (kSaThreads / 32);   // 32-row segments per warp in the rank passes
 constexpr int kSegB = 8;                                  // segments whose loads a rank pass batches
 static_assert(kSegW % kSegB == 0 && kSegB <= 32, "rank passes take whole batches");
+constexpr int kLowGroups = 2;   // 32-leaf groups a warp takes through the warp-local levels at once
 constexpr int kWalkSpanMax = 64;   // walks crossing more columns are taken by a whole warp
 
 static_assert(kSaSB / kSaSF <= kSaThreads - 32, "the walk phase needs at least one warp without a thread walk");
@@ -285,77 +286,126 @@ __device__ __forceinline__ void warp_walk(SaShared &S, int a, int k, int top, in
 // L(r) = #{lo points in rows >= r} = -delta(r, 0), c*(r) - 1 is the column of the L(r)-th column g of the node
 // whose point raises delta in row r (one ballot per row of the node: bit g = colind(g, r)); the lists are
 // reordered through the group's slice of PL / QL.  Only __syncwarp: nothing here is shared with other warps.
-__device__ __forceinline__ void warp_low_levels(SaShared &S, int o, int cnt, int lane) {
-    int pl = lane < cnt ? S.PL[o + lane] : INT_MAX;
-    int ql = lane < cnt ? S.QL[o + lane] : INT_MAX;
-    int res = 0;
+// NG groups at once (o, o + 32, ...; group j holds cnt[j] <= 32 leaves, 0 for none): the groups' steps are
+// independent, so interleaving them hides the shuffle and shared-memory latencies of each.
+template <int NG>
+__device__ __forceinline__ void warp_low_levels(SaShared &S, int o, const int (&cnt)[NG], int lane) {
+    int pl[NG], ql[NG], res[NG];
+    int cmax = 0;
+#pragma unroll
+    for (int j = 0; j < NG; ++j) {
+        pl[j] = lane < cnt[j] ? S.PL[o + 32 * j + lane] : INT_MAX;
+        ql[j] = lane < cnt[j] ? S.QL[o + 32 * j + lane] : INT_MAX;
+        res[j] = 0;
+        cmax = max(cmax, cnt[j]);
+    }
 #pragma unroll
     for (int h = 1; h < 32; h <<= 1) {
-        if (h >= cnt) break;
+        if (h >= cmax) break;
         const int s = 2 * h;
         const int a = lane & ~(s - 1);
-        const int m = min(a + h, cnt), b = min(a + s, cnt);
-        const bool two = lane < cnt && m < b;   // the lane's node has both children
-        const bool lo = lane < m;
-        // parent positions in the row-id (PL) and column-id (QL) merges: the number of sibling entries below
-        // the lane's own (entries are distinct), by binary lifting over the sibling's sorted lanes [sb, se)
-        const int sb = lo ? m : a, len = lo ? b - m : m - a;
-        int cp = 0, cq = 0;
+        int m[NG], b[NG], pp[NG], pq[NG];
+        bool two[NG], lo[NG];
 #pragma unroll
-        for (int step = h; step >= 1; step >>= 1) {
-            const int vp = __shfl_sync(kFull, pl, (sb + cp + step - 1) & 31);
-            const int vq = __shfl_sync(kFull, ql, (sb + cq + step - 1) & 31);
-            if (cp + step <= len && vp < pl) cp += step;
-            if (cq + step <= len && vq < ql) cq += step;
+        for (int j = 0; j < NG; ++j) {
+            m[j] = min(a + h, cnt[j]);
+            b[j] = min(a + s, cnt[j]);
+            two[j] = lane < cnt[j] && m[j] < b[j];   // the lane's node has both children
+            lo[j] = lane < m[j];
         }
-        const int base = lo ? lane - a : lane - m;
-        const int pp = two ? base + cp : lane - a;
-        const int pq = two ? base + cq : lane - a;
+        // parent positions in the row-id (PL) and column-id (QL) merges: the number of sibling entries below
+        // the lane's own (entries are distinct), by binary lifting over the sibling's sorted lanes
+        {
+            int sb[NG], len[NG], cp[NG], cq[NG];
+#pragma unroll
+            for (int j = 0; j < NG; ++j) {
+                sb[j] = lo[j] ? m[j] : a;
+                len[j] = lo[j] ? b[j] - m[j] : m[j] - a;
+                cp[j] = cq[j] = 0;
+            }
+#pragma unroll
+            for (int step = h; step >= 1; step >>= 1) {
+#pragma unroll
+                for (int j = 0; j < NG; ++j) {
+                    const int vp = __shfl_sync(kFull, pl[j], (sb[j] + cp[j] + step - 1) & 31);
+                    const int vq = __shfl_sync(kFull, ql[j], (sb[j] + cq[j] + step - 1) & 31);
+                    if (cp[j] + step <= len[j] && vp < pl[j]) cp[j] += step;
+                    if (cq[j] + step <= len[j] && vq < ql[j]) cq[j] += step;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NG; ++j) {
+                const int base = lo[j] ? lane - a : lane - m[j];
+                pp[j] = two[j] ? base + cp[j] : lane - a;
+                pq[j] = two[j] ? base + cq[j] : lane - a;
+            }
+        }
         // the child's product (row -> child-local col) in the parent's coordinates
-        const int cs = lo ? a : m;
-        const int col = __shfl_sync(kFull, pq, (cs + res) & 31);
-        if (two) {
-            S.xs[o + a + pp] = (uint16_t) (col | (lo ? 0 : 0x8000));
-            S.ys[o + a + col] = (uint16_t) (pp | (lo ? 0 : 0x8000));
+#pragma unroll
+        for (int j = 0; j < NG; ++j) {
+            const int cs = lo[j] ? a : m[j];
+            const int col = __shfl_sync(kFull, pq[j], (cs + res[j]) & 31);
+            if (two[j]) {
+                S.xs[o + 32 * j + a + pp[j]] = (uint16_t) (col | (lo[j] ? 0 : 0x8000));
+                S.ys[o + 32 * j + a + col] = (uint16_t) (pp[j] | (lo[j] ? 0 : 0x8000));
+            }
         }
         __syncwarp();
-        const int x = two ? S.xs[o + lane] : 0;
-        const int y = two ? S.ys[o + lane] : 0;
+        int x[NG], y[NG];
+#pragma unroll
+        for (int j = 0; j < NG; ++j) {
+            x[j] = two[j] ? S.xs[o + 32 * j + lane] : 0;
+            y[j] = two[j] ? S.ys[o + 32 * j + lane] : 0;
+        }
         // c*(r) = min{c : delta(r, c) >= 0}, delta(r, 0) = -#{lo points in rows >= r}
-        const int k = b - a, r = lane - a;
-        const unsigned lomask = __ballot_sync(kFull, two && !(x >> 15));
-        const unsigned upto = b >= 32 ? 0xffffffffu : ((1u << b) - 1u);
-        const int need = __popc(lomask & upto & ~((1u << lane) - 1u));
-        const int yr = y & 0x7fff;
-        const bool yhi = y >> 15;
-        unsigned mine = 0u;   // bit g: colind(g, r) for the columns g of the lane's node, row r = lane - a
+        const int r = lane - a;
+        unsigned mine[NG];   // bit g: colind(g, r) for the columns g of the lane's node, row r = lane - a
+#pragma unroll
+        for (int j = 0; j < NG; ++j) mine[j] = 0u;
 #pragma unroll
         for (int i = 0; i < s; ++i) {
-            const unsigned M = __ballot_sync(kFull, two && (yhi ? (yr < i) : (yr >= i)));
-            if (r == i) mine = M;
+#pragma unroll
+            for (int j = 0; j < NG; ++j) {
+                const int yr = y[j] & 0x7fff;
+                const unsigned M = __ballot_sync(kFull, two[j] && ((y[j] >> 15) ? (yr < i) : (yr >= i)));
+                if (r == i) mine[j] = M;
+            }
         }
-        mine = (mine >> a) & (k >= 32 ? 0xffffffffu : ((1u << k) - 1u));
-        const int cstar = need == 0 ? 0 : (__popc(mine) >= need ? (int) __fns(mine, 0, need) + 1 : k + 1);
-        if (two) {
-            const int xr = x & 0x7fff;
-            const bool hi = x >> 15;
-            const bool good = cstar >= 1 && cstar <= k && (hi ? (xr < cstar) : (xr >= cstar));
-            res = good ? cstar - 1 : xr;
+#pragma unroll
+        for (int j = 0; j < NG; ++j) {
+            const int k = b[j] - a;
+            const unsigned lomask = __ballot_sync(kFull, two[j] && !(x[j] >> 15));
+            const unsigned upto = b[j] >= 32 ? 0xffffffffu : ((1u << b[j]) - 1u);
+            const int need = __popc(lomask & upto & ~((1u << lane) - 1u));
+            const unsigned mk = (mine[j] >> a) & (k >= 32 ? 0xffffffffu : ((1u << k) - 1u));
+            const int cstar = need == 0 ? 0 : (__popc(mk) >= need ? (int) __fns(mk, 0, need) + 1 : k + 1);
+            if (two[j]) {
+                const int xr = x[j] & 0x7fff;
+                const bool hi = x[j] >> 15;
+                const bool good = cstar >= 1 && cstar <= k && (hi ? (xr < cstar) : (xr >= cstar));
+                res[j] = good ? cstar - 1 : xr;
+            }
         }
         // the lists in the parent's order
         __syncwarp();
-        if (two) {
-            S.PL[o + a + pp] = pl;
-            S.QL[o + a + pq] = ql;
-        }
+#pragma unroll
+        for (int j = 0; j < NG; ++j)
+            if (two[j]) {
+                S.PL[o + 32 * j + a + pp[j]] = pl[j];
+                S.QL[o + 32 * j + a + pq[j]] = ql[j];
+            }
         __syncwarp();
-        if (two) {
-            pl = S.PL[o + lane];
-            ql = S.QL[o + lane];
-        }
+#pragma unroll
+        for (int j = 0; j < NG; ++j)
+            if (two[j]) {
+                pl[j] = S.PL[o + 32 * j + lane];
+                ql[j] = S.QL[o + 32 * j + lane];
+            }
         __syncwarp();
     }
-    if (lane < cnt) S.RES[o + lane] = (uint16_t) res;
+#pragma unroll
+    for (int j = 0; j < NG; ++j)
+        if (lane < cnt[j]) S.RES[o + 32 * j + lane] = (uint16_t) res[j];
     __syncwarp();
 }
 
@@ -376,7 +426,12 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
     }
     __syncthreads();
     // spans 2..32: one warp per 32-leaf group
-    for (int o = warp * 32; o < nb; o += nwarps * 32) warp_low_levels(S, o, min(32, nb - o), lane);
+    for (int o = warp * 32 * kLowGroups; o < nb; o += nwarps * 32 * kLowGroups) {
+        int cnt[kLowGroups];
+#pragma unroll
+        for (int j = 0; j < kLowGroups; ++j) cnt[j] = max(0, min(32, nb - o - 32 * j));
+        warp_low_levels<kLowGroups>(S, o, cnt, lane);
+    }
     __syncthreads();
     for (int size = 32; size < nb; size <<= 1) {
         const int span = size << 1;

@@ -39,6 +39,15 @@ def test_mid_sizes(engine, oracle, n):
     assert np.array_equal(engine.steady_ant(p, q), oracle.steady_ant(p, q))
 
 
+@pytest.mark.parametrize("cutoff", [1024, 2048, 4096])
+def test_cutoffs_and_partial_nodes(engine, oracle, cutoff):
+    """Every shared-memory subtree size the tuner may pick; sizes whose last node at each span has one child, two
+    unequal children, or exactly fills it (the walked spans below 1024 and the ranked spans from 1024 up)."""
+    for n in [1536, 1537, 2047, 2049, 3000, 3071, 6143, 12289, 20000]:
+        p, q = gen.permutation(n, 710 + n % 7, n), gen.permutation(n, 711 + n % 5, n)
+        assert np.array_equal(engine.steady_ant(p, q, sa_cutoff=cutoff), oracle.steady_ant(p, q)), (n, cutoff)
+
+
 def test_large_properties(engine, oracle):
     """2^22 (the headline size): exact against the sequential oracle (a few seconds on the host)."""
     n = 1 << 22
