@@ -153,6 +153,27 @@ int slcs_window_scores(const int32_t *row_to_col, int m, int n, int w, int32_t *
 int slcs_window_scores_dev(const int32_t *d_row_to_col, const int32_t *d_col_to_row, int m, int n, int w,
                            int32_t *d_out, void *stream);
 
+/* ---- approximate pattern search ----------------------------------------------------------------- */
+/* An interval [start, end) of the text and its score: minus the indel distance (substitution = 2 indels) of the
+ * pattern and the interval, the reference's approximate_matching::utils::Interval
+ * (R:approximate_matching/utils.h:233-253) with the fixed scoring scheme (0, -2, -1). */
+typedef struct slcs_interval {
+    int32_t start;
+    int32_t end;
+    double score;
+} slcs_interval;
+
+/* Approximate copies of `pattern` (m symbols) in `text` (n >= int(m / k) symbols), 0 < k <= 1: replaces
+ * InteractiveDuplicateSearchSemiDense::find (R:approximate_matching/ApproximateMatching.h:320-420) with the same
+ * result vector.  One braid of the pattern against the text (the combing engine), every window's score by the
+ * window scan, every window's best interval by a warp kernel; the dedup, sort and greedy pick on the host.
+ * Writes the first min(count, out_cap) intervals to out and the count to *n_out.  SLCS_ERR_ARG for a text shorter
+ * than the window, SLCS_ERR_TOO_LARGE for a window of more than 16384 interval ends or 2^21 symbols. */
+int slcs_duplicate_search_u8(const uint8_t *pattern, int m, const uint8_t *text, int n, double k, slcs_interval *out,
+                             int out_cap, int *n_out);
+int slcs_duplicate_search_i32(const int32_t *pattern, int m, const int32_t *text, int n, double k,
+                              slcs_interval *out, int out_cap, int *n_out);
+
 /* ---- batched combing -------------------------------------------------------------------------- */
 /* Braids of npairs independent pairs in one persistent, length-bucketed launch.  a_cat / b_cat hold the
  * concatenated symbols, a_off / b_off (npairs) the start of each string, m / n (npairs) the lengths;

@@ -22,6 +22,11 @@ mkdir -p "$here/_ref"
   -I"$src" "$here/ref_shim.cpp" -o "$here/_ref/libslcs_ref.so.tmp" -Wl,--no-undefined
 mv "$here/_ref/libslcs_ref.so.tmp" "$here/_ref/libslcs_ref.so"
 echo "build_ref: wrote $here/_ref/libslcs_ref.so"
+# The approximate pattern search (legacy permutation types: its own library)
+/usr/bin/g++ -std=c++17 -O3 -march=x86-64-v3 -fPIC -shared -w \
+  -I"$src" "$here/ref_am_shim.cpp" -o "$here/_ref/libslcs_ref_am.so.tmp" -Wl,--no-undefined
+mv "$here/_ref/libslcs_ref_am.so.tmp" "$here/_ref/libslcs_ref_am.so"
+echo "build_ref: wrote $here/_ref/libslcs_ref_am.so"
 # Two of the reference's own benchmark executables (its harness protocol: R:utils/runners.py), as the pin of the
 # harness runners in semilocal_b200/harness/.
 for f in semi_local_naive_iterative semi_local_hybrid_iterative; do

@@ -3,7 +3,8 @@
 Two libraries are wrapped:
   * liboracle.so   -- the C restatement in oracle/slcs_oracle.c (always built; `make -C oracle`);
   * _ref/libslcs_ref.so -- the reference's own headers compiled by oracle/build_ref.sh (present when the
-    reference sources were available at build time; the file travels with the repository snapshot).
+    reference sources were available at build time; the file travels with the repository snapshot);
+  * _ref/libslcs_ref_am.so -- the reference's approximate pattern search, compiled the same way.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may import this module.
 """
@@ -19,6 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libslcs_ref.so")
+REF_AM_PATH = os.path.join(HERE, "_ref", "libslcs_ref_am.so")
 
 _lock = threading.Lock()
 _lib = None
@@ -27,12 +29,14 @@ _ref_tried = False
 
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_ref_am = None
 
 
 def build() -> str:
-    """(Re)build liboracle.so if it is missing or older than its source."""
-    src = os.path.join(HERE, "slcs_oracle.c")
-    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+    """(Re)build liboracle.so if it is missing or older than its sources."""
+    srcs = [os.path.join(HERE, f) for f in ("slcs_oracle.c", "amatch_oracle.cpp")]
+    if not os.path.exists(LIB_PATH) or any(os.path.getmtime(LIB_PATH) < os.path.getmtime(f) for f in srcs):
         subprocess.run(["make", "-C", HERE, "-s"], check=True)
     return LIB_PATH
 
@@ -61,6 +65,8 @@ def lib():
             L.slo_bit_llcs_nary_u64.argtypes = [_u64p, ctypes.c_int, _u64p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
             L.slo_bit_llcs_binary_u64.argtypes = [_u64p, ctypes.c_int, _u64p, ctypes.c_int, ctypes.c_int]
             L.slo_comb_score.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int]
+            L.slo_duplicate_search.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_double, _i32p, _i32p,
+                                               _f64p, ctypes.c_int]
             _lib = L
     return _lib
 
@@ -322,3 +328,41 @@ def ref_bit_binary(a, b, threads: int = 1) -> int:
     R = ref()
     a, b = _i32(a), _i32(b)
     return int(R.ref_bit_binary_u64(_p(a), len(a), _p(b), len(b), threads))
+
+
+# --------------------------------------------------------------------------------------------------
+# Approximate pattern search: the restatement and the reference's own code
+# --------------------------------------------------------------------------------------------------
+
+def _intervals(fn, pattern, text, k):
+    p, t = _i32(pattern), _i32(text)
+    cap = max(len(t), 1)
+    st, en = np.empty(cap, np.int32), np.empty(cap, np.int32)
+    sc = np.empty(cap, np.float64)
+    cnt = fn(_p(p), len(p), _p(t), len(t), ctypes.c_double(k), _p(st), _p(en), sc.ctypes.data_as(_f64p), cap)
+    if cnt < 0:
+        raise ValueError("bad arguments")
+    return [(int(st[i]), int(en[i]), float(sc[i])) for i in range(cnt)]
+
+
+def duplicate_search(pattern, text, k: float):
+    """The restatement of InteractiveDuplicateSearchSemiDense::find (oracle/amatch_oracle.cpp)."""
+    return _intervals(lib().slo_duplicate_search, pattern, text, k)
+
+
+def ref_am():
+    """The reference-compiled approximate pattern search, or None when it was not built."""
+    global _ref_am
+    with _lock:
+        if _ref_am is None and os.path.exists(REF_AM_PATH):
+            R = ctypes.CDLL(REF_AM_PATH)
+            for f in (R.ref_dup_search_dense, R.ref_dup_search_sparse):
+                f.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_double, _i32p, _i32p, _f64p, ctypes.c_int]
+            _ref_am = R
+    return _ref_am
+
+
+def ref_duplicate_search(pattern, text, k: float, kind: str = "dense"):
+    """The reference's own InteractiveDuplicateSearchSemiDense (kind "dense") or ...SemiSparse ("sparse")."""
+    R = ref_am()
+    return _intervals(R.ref_dup_search_dense if kind == "dense" else R.ref_dup_search_sparse, pattern, text, k)

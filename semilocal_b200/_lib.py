@@ -51,6 +51,11 @@ class Result(ctypes.Structure):
                 ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double)]
 
 
+class Interval(ctypes.Structure):
+    """slcs_interval: [start, end) of the text and its score."""
+    _fields_ = [("start", ctypes.c_int32), ("end", ctypes.c_int32), ("score", ctypes.c_double)]
+
+
 class ServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int64) for k in ("submitted", "completed", "rejected", "evicted", "resident",
                                              "resident_bytes", "used_bytes", "peak_bytes", "budget", "launches",
@@ -119,6 +124,8 @@ SIGNATURES = {
     "slcs_server_destroy": [_vp],
     "slcs_window_scores": [_i32p, _int, _int, _int, _i32p],
     "slcs_window_scores_dev": [_vp, _vp, _int, _int, _int, _vp, _vp],
+    "slcs_duplicate_search_u8": [_u8p, _int, _u8p, _int, ctypes.c_double, ctypes.POINTER(Interval), _int, _i32p],
+    "slcs_duplicate_search_i32": [_i32p, _int, _i32p, _int, ctypes.c_double, ctypes.POINTER(Interval), _int, _i32p],
     "slcs_server_window": [_vp, ctypes.c_uint64, _int, _i32p],
     "slcs_selftest_wait_timeout": [_i32p],
     "slcs_check_permutation": [_i32p, _int, _i32p],

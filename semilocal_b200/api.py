@@ -145,6 +145,25 @@ def window_scores(row_to_col, m: int, n: int, w: int) -> np.ndarray:
     return out[:max(n - w + 1, 0)]
 
 
+def duplicate_search(pattern, text, k: float) -> List[Tuple[int, int, float]]:
+    """Approximate copies of `pattern` in `text` as (start, end, score) intervals: the result vector of the
+    reference's InteractiveDuplicateSearchSemiDense::find (R:approximate_matching/ApproximateMatching.h:320-420)
+    for the same symbols and k (0 < k <= 1), computed from one braid on the device."""
+    p = np.asarray(pattern)
+    t = np.asarray(text)
+    if p.dtype == np.uint8 and t.dtype == np.uint8:
+        fn, ptr = lib().slcs_duplicate_search_u8, _u8p
+    else:
+        p, t = p.astype(np.int32), t.astype(np.int32)
+        fn, ptr = lib().slcs_duplicate_search_i32, _i32p
+    p, t = np.ascontiguousarray(p), np.ascontiguousarray(t)
+    cap = max(len(t) - int(len(p) / k) + 2, 1) if k > 0 else 1
+    out = (_lib.Interval * cap)()
+    cnt = ctypes.c_int32(0)
+    check(fn(_p(p, ptr), len(p), _p(t, ptr), len(t), ctypes.c_double(k), out, cap, ctypes.byref(cnt)))
+    return [(out[i].start, out[i].end, out[i].score) for i in range(min(cnt.value, cap))]
+
+
 def scores(row_to_col, m: int, n: int, queries: Sequence[Tuple[int, int, int]]) -> np.ndarray:
     """Answer (kind, i, j) queries against a braid; see SLCS_Q_* in include/slcs.h."""
     r2c = np.ascontiguousarray(row_to_col, dtype=np.int32)

@@ -157,6 +157,8 @@ bool use_hybrid(const slcs_opts *opts, int m, int n) {
     return false;   // AUTO: the wavefront saturates the device once the pair has ~1000 bands; see DESIGN
 }
 
+}  // namespace
+
 template <typename T>
 int comb_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int32_t *d_r2c, int32_t *d_c2r, int32_t *d_score,
              const slcs_opts *opts, cudaStream_t s) {
@@ -164,6 +166,12 @@ int comb_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int32_t *d_r2c
     if (use_hybrid(opts, m, n)) return comb_hybrid_dev<T>(E, d_a, m, d_b, n, d_r2c, d_c2r, d_score, opts, s);
     return comb_wavefront_dev<T>(E, d_a, m, d_b, n, d_r2c, d_c2r, d_score, opts, s);
 }
+template int comb_dev<uint8_t>(Engine *, const uint8_t *, int, const uint8_t *, int, int32_t *, int32_t *, int32_t *,
+                               const slcs_opts *, cudaStream_t);
+template int comb_dev<int32_t>(Engine *, const int32_t *, int, const int32_t *, int, int32_t *, int32_t *, int32_t *,
+                               const slcs_opts *, cudaStream_t);
+
+namespace {
 
 int identity_host(int size, int32_t *r2c, int32_t *c2r, int32_t *score) {
     for (int i = 0; i < size; ++i) {

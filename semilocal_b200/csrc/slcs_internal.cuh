@@ -263,6 +263,10 @@ int launch_scores(const int32_t *d_r2c, int m, int n, const slcs_query *d_q, int
                   cudaStream_t s);
 // LCS(a, b[s..s+w)) for every window s = 0..n-w of a braid (d_c2r optional: computed when NULL); synchronous.
 int window_scores_dev(const int32_t *d_r2c, const int32_t *d_c2r, int m, int n, int w, int32_t *d_out, cudaStream_t s);
+// The braid of one pair on the device (capi.cu): wavefront, or the hybrid when opts ask for it.
+template <typename T>
+int comb_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int32_t *d_r2c, int32_t *d_c2r, int32_t *d_score,
+             const slcs_opts *opts, cudaStream_t s);
 // The same for host queries / answers (synchronous on s).
 int launch_scores_host(const int32_t *d_r2c, int m, int n, const slcs_query *q, int nq, int32_t *out,
                        cudaStream_t s);

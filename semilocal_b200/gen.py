@@ -114,6 +114,19 @@ def batch_pairs(count: int = 4096, lo: int = 256, hi: int = 65536, seed: int = 5
     return pairs
 
 
+def planted_text(m: int, n: int, copies: int, alphabet: int = 4, seed: int = 0, subst: float = 0.1,
+                 indel: float = 0.02):
+    """Approximate pattern search input: a pattern of m uniform symbols and a text of n uniform symbols overwritten
+    at `copies` seeded positions by mutated copies of the pattern (substitutions, half insertions, half deletions)."""
+    p = uniform_string(m, alphabet, seed, 1)
+    t = uniform_string(n, alphabet, seed, 2).copy()
+    pos = (uniform01(seed, copies, 3) * max(1, n - m)).astype(np.int64)
+    for c, at in enumerate(pos):
+        seg = mutate(p, subst, indel / 2, indel / 2, alphabet, seed * 1000 + c)[:max(0, n - int(at))]
+        t[int(at):int(at) + len(seg)] = seg
+    return p, t
+
+
 def serving_requests(count: int, rate_hz: float, lo: int = 1000, hi: int = 1_000_000, seed: int = 6):
     """Poisson arrivals at `rate_hz`; each request a pair with log-uniform length and a query kind
     uniform over {global, string-substring, prefix-suffix}.  Returns a list of dicts."""
