@@ -453,8 +453,41 @@ def run_suite(torch, S, peak_cells, peaks):
                           "bit_gcups": round(len(tbit_a) * len(tbit_b) / tb / 1e9, 2),
                           "bit_sample": "llcs_nary_symbol_smart_combing<uint64_t>, 2 bits/symbol, leading 2^17 x 2^17"}
     out["hybrid_pair_2p20"] = res
+    out["approximate_search"] = run_approximate_search(S, O, use_ref)
     out["serving"] = run_serving(S, O, use_ref, ncpu)
     return out
+
+
+def run_approximate_search(S, O, use_ref):
+    """Approximate copies of a 1000-symbol pattern in a 2^22-symbol text (4 letters, 200 planted copies with 10 %
+    substitutions and 2 % indels), k = 0.9, through the public call (host buffers in, intervals out): the dense and
+    the sparse search.  The reference's own searches run on a bounded sample, the leading 2^18 (dense) or 2^16
+    (sparse) symbols of the text, and the GPU result on that sample is compared with theirs."""
+    p, t = gen.planted_text(1000, 1 << 22, 200, 4, 31)
+    k = 0.9
+    res = {"pattern": len(p), "text": len(t), "k": k, "cells": len(p) * len(t)}
+    for name, sparse in (("dense", False), ("sparse", True)):
+        S.duplicate_search(p, t, k, sparse=sparse)   # warm-up
+        times = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            found = S.duplicate_search(p, t, k, sparse=sparse)
+            times.append(time.perf_counter() - t0)
+        best = min(times)
+        ent = {"e2e_ms": round(best * 1e3, 2), "intervals": len(found),
+               "gcups_e2e": round(len(p) * len(t) / best / 1e9, 1)}
+        ts = t[:1 << (16 if sparse else 18)]   # the reference's sparse search spends ~90 us per symbol
+        if use_ref and O.ref_am() is not None:
+            t0 = time.perf_counter()
+            ref = O.ref_duplicate_search(p, ts, k, "sparse" if sparse else "dense")
+            rt = time.perf_counter() - t0
+            ent["equal_to_reference_on_sample"] = S.duplicate_search(p, ts, k, sparse=sparse) == ref
+            ent["cpu_ref"] = {"kind": "reference", "threads": 1,
+                              "sample": f"leading {len(ts)} symbols of the text",
+                              "seconds": round(rt, 3), "gcups": round(len(p) * len(ts) / rt / 1e9, 3),
+                              "impl": "InteractiveDuplicateSearchSemi" + ("Sparse" if sparse else "Dense") + "::find"}
+        res[name] = ent
+    return res
 
 
 def _serving_query(r):

@@ -22,6 +22,8 @@
  *   lcs::LCSStrategy<Input>::compute                        R:include/LCS/LCS.h:9-13
  *   prefix_lcs_via_semi_local::nary::llcs_nary_symbol_smart_combing
  *                                                           R:prefix_lcs/bitwise/transposition_network_binary_alphabet.h:668-736
+ *   InteractiveDuplicateSearchSemiDense / ...SemiSparse::find
+ *                                                           R:approximate_matching/ApproximateMatching.h:252-420
  */
 #ifndef SLCS_H
 #define SLCS_H
@@ -173,6 +175,14 @@ int slcs_duplicate_search_u8(const uint8_t *pattern, int m, const uint8_t *text,
                              int out_cap, int *n_out);
 int slcs_duplicate_search_i32(const int32_t *pattern, int m, const int32_t *text, int n, double k,
                               slcs_interval *out, int out_cap, int *n_out);
+/* The same search with the reference's InteractiveDuplicateSearchSemiSparse::find
+ * (R:approximate_matching/ApproximateMatching.h:252-318): only the windows its first phase visits (it skips ahead
+ * by half the score deficit) are clones; each clone's best interval is the one the dense search finds for that
+ * window start (the reference reads it from the clone's own braid). */
+int slcs_duplicate_search_sparse_u8(const uint8_t *pattern, int m, const uint8_t *text, int n, double k,
+                                    slcs_interval *out, int out_cap, int *n_out);
+int slcs_duplicate_search_sparse_i32(const int32_t *pattern, int m, const int32_t *text, int n, double k,
+                                     slcs_interval *out, int out_cap, int *n_out);
 
 /* ---- batched combing -------------------------------------------------------------------------- */
 /* Braids of npairs independent pairs in one persistent, length-bucketed launch.  a_cat / b_cat hold the

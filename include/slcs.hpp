@@ -208,6 +208,34 @@ public:
     }
 };
 
+// An interval of the text and its score, the fields of the reference's approximate_matching::utils::Interval
+// (R:approximate_matching/utils.h:233-253).
+struct Interval {
+    int start;
+    int end;
+    double score;
+    int len() const { return end - start; }
+};
+
+// InteractiveDuplicateSearchSemiDense / ...SemiSparse shape (R:approximate_matching/ApproximateMatching.h:252-420):
+// find(p, p_size, text, text_size, k, result) appends the same intervals the reference's find does.
+template <bool Sparse>
+class GpuDuplicateSearch {
+public:
+    template <class T>
+    void find(const T *p, int p_size, const T *text, int text_size, double k, std::vector<Interval> &result) const {
+        std::vector<int32_t> pp(p, p + p_size), tt(text, text + text_size);
+        const int cap = text_size + 1;
+        std::vector<slcs_interval> out(cap);
+        int cnt = 0;
+        check(Sparse ? slcs_duplicate_search_sparse_i32(pp.data(), p_size, tt.data(), text_size, k, out.data(), cap, &cnt)
+                     : slcs_duplicate_search_i32(pp.data(), p_size, tt.data(), text_size, k, out.data(), cap, &cnt));
+        for (int i = 0; i < cnt && i < cap; ++i) result.push_back(Interval{out[i].start, out[i].end, out[i].score});
+    }
+};
+using GpuDuplicateSearchSemiDense = GpuDuplicateSearch<false>;
+using GpuDuplicateSearchSemiSparse = GpuDuplicateSearch<true>;
+
 // Scores read from a braid: SLCS_Q_* queries (global, string-substring, prefix-suffix, ...).
 template <class Perm>
 std::vector<int32_t> scores(const Perm &braid, const std::vector<slcs_query> &qs) {

@@ -1,5 +1,6 @@
 // amatch_oracle.cpp -- TEST INFRASTRUCTURE ONLY: host restatement of the reference's approximate pattern search,
-// InteractiveDuplicateSearchSemiDense::find (R:approximate_matching/ApproximateMatching.h:320-420), step for step:
+// InteractiveDuplicateSearchSemiDense::find (R:approximate_matching/ApproximateMatching.h:320-420), step for step
+// (and ...SemiSparse::find, :252-318, further down):
 //   * one braid of the pattern against the text (row-major combing, slo_comb_rowmajor in slcs_oracle.c);
 //   * the triangle of the last window (calculateTriangle, ApproximateMatching.h:137-184): for each interval end
 //     j = n - kk, the best interval over starts walking down the column;
@@ -11,6 +12,7 @@
 // R:unit_monge_mult/dominance_sum_queries.h:84-118.  C++ because the pick sorts with std::sort, whose order of
 // equal keys the result depends on.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <unordered_set>
 #include <vector>
@@ -35,6 +37,86 @@ bool better(const Iv &a, const Iv &b) {
 }
 
 }  // namespace
+
+// The greedy pick (phase3, ApproximateMatching.h:186-200); returns the number of intervals, writing at most cap.
+static int pick(std::vector<Iv> &cands, int32_t *starts, int32_t *ends, double *scores, int cap) {
+    std::sort(cands.begin(), cands.end(), [](const Iv &a, const Iv &b) {
+        return (a.start < b.start) || (a.start == b.start && a.score > b.score);
+    });
+    int lb = 0, rb = 0, cnt = 0;
+    for (const Iv &c : cands) {
+        if (c.start > lb && c.start >= rb) {
+            if (cnt < cap) {
+                starts[cnt] = c.start;
+                ends[cnt] = c.end;
+                scores[cnt] = c.score;
+            }
+            ++cnt;
+            lb = c.start;
+            rb = std::max(rb, c.end);
+        }
+    }
+    return cnt;
+}
+
+// The edit distance of the reference's first phase (DuplicateSearch::editDistance, ApproximateMatching.h:18-53):
+// match 0, substitution 2, indel 1, negated.
+static double edit_score(const int32_t *a, int na, const int32_t *b, int nb) {
+    std::vector<double> prev(nb + 1), cur(nb + 1);
+    for (int j = 0; j <= nb; ++j) prev[j] = j;
+    for (int i = 1; i <= na; ++i) {
+        cur[0] = i;
+        for (int j = 1; j <= nb; ++j)
+            cur[j] = std::min(a[i - 1] == b[j - 1] ? prev[j - 1] : 2.0 + prev[j - 1], 1.0 + std::min(prev[j], cur[j - 1]));
+        std::swap(prev, cur);
+    }
+    return -prev[nb];
+}
+
+// InteractiveDuplicateSearchSemiSparse::find (ApproximateMatching.h:252-318): the first phase walks the window ends,
+// skipping ahead by half the score deficit; each clone (a window scoring at least kdi) is combed against the
+// pattern on its own and its triangle (calculateTriangle, offset 0, the whole clone) gives the clone's interval.
+extern "C" int slo_duplicate_search_sparse(const int32_t *p, int m, const int32_t *t, int n, double k,
+                                           int32_t *starts, int32_t *ends, double *scores, int cap) {
+    if (m <= 0 || n <= 0 || !(k > 0.0 && k <= 1.0)) return -1;
+    const int w = int(m / k);
+    const int left_w = int(m * k) - 1;
+    const double kdi = -(m * (1 / k + 1) * (1 - k * k));
+    if (w > n) return -1;
+    std::vector<Iv> clones;
+    for (int end = w; end < n + 1;) {
+        const double dist = edit_score(t + (end - w), w, p, m);
+        if (dist >= kdi) clones.push_back(Iv{end - w, end, dist});
+        if (dist < kdi - 1) end += std::max(1, int((std::abs(dist) - std::abs(kdi)) / 2));
+        else ++end;
+    }
+    std::vector<Iv> cands;
+    std::unordered_set<long long> seen;
+    std::vector<int32_t> r2c(m + w), c2r(m + w);
+    for (const Iv &cl : clones) {
+        slo_comb_rowmajor(p, m, t + cl.start, w, r2c.data());
+        for (int s = 0; s < m + w; ++s) c2r[r2c[s]] = s;
+        // D(0, w) of the clone from its score: w - LCS, LCS = (score + m + w) / 2 (getRangeSumFromReverse)
+        int dcol = static_cast<int>(std::lround(w - (cl.score + m + w) / 2.0));
+        Iv wmax{0, 0, kNegInf};
+        for (int kk = 0; kk < w - left_w; ++kk) {
+            const int j = w - kk;
+            int d = dcol;
+            Iv best{0, 0, kNegInf};
+            for (int tt = 0; tt < (w - kk) - left_w; ++tt) {
+                const Iv c{tt, j, 2.0 * (j - tt - d) - (m + j - tt)};
+                if (c.score > best.score || (c.score == best.score && c.len() > best.len())) best = c;
+                if (r2c[m + tt] < j) --d;
+            }
+            if (better(best, wmax)) wmax = best;
+            if (c2r[j - 1] >= m) --dcol;
+        }
+        const Iv shifted{wmax.start + cl.start, wmax.end + cl.start, wmax.score};
+        const long long key = (static_cast<long long>(shifted.start) << 32) | static_cast<unsigned>(shifted.end);
+        if (seen.insert(key).second) cands.push_back(shifted);
+    }
+    return pick(cands, starts, ends, scores, cap);
+}
 
 // Returns the number of intervals (writing at most cap of them), -1 for bad arguments.
 extern "C" int slo_duplicate_search(const int32_t *p, int m, const int32_t *t, int n, double k, int32_t *starts,
@@ -109,23 +191,5 @@ extern "C" int slo_duplicate_search(const int32_t *p, int m, const int32_t *t, i
         diag = up(m + i, j - 1, diag);
     }
     std::reverse(cands.begin(), cands.end());
-
-    // ---- phase 3: the greedy pick ----
-    std::sort(cands.begin(), cands.end(), [](const Iv &a, const Iv &b) {
-        return (a.start < b.start) || (a.start == b.start && a.score > b.score);
-    });
-    int lb = 0, rb = 0, cnt = 0;
-    for (const Iv &c : cands) {
-        if (c.start > lb && c.start >= rb) {
-            if (cnt < cap) {
-                starts[cnt] = c.start;
-                ends[cnt] = c.end;
-                scores[cnt] = c.score;
-            }
-            ++cnt;
-            lb = c.start;
-            rb = std::max(rb, c.end);
-        }
-    }
-    return cnt;
+    return pick(cands, starts, ends, scores, cap);
 }

@@ -67,6 +67,7 @@ def lib():
             L.slo_comb_score.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int]
             L.slo_duplicate_search.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_double, _i32p, _i32p,
                                                _f64p, ctypes.c_int]
+            L.slo_duplicate_search_sparse.argtypes = L.slo_duplicate_search.argtypes
             _lib = L
     return _lib
 
@@ -345,9 +346,10 @@ def _intervals(fn, pattern, text, k):
     return [(int(st[i]), int(en[i]), float(sc[i])) for i in range(cnt)]
 
 
-def duplicate_search(pattern, text, k: float):
-    """The restatement of InteractiveDuplicateSearchSemiDense::find (oracle/amatch_oracle.cpp)."""
-    return _intervals(lib().slo_duplicate_search, pattern, text, k)
+def duplicate_search(pattern, text, k: float, sparse: bool = False):
+    """The restatement of InteractiveDuplicateSearchSemiDense::find, or ...SemiSparse::find with sparse=True
+    (oracle/amatch_oracle.cpp)."""
+    return _intervals(lib().slo_duplicate_search_sparse if sparse else lib().slo_duplicate_search, pattern, text, k)
 
 
 def ref_am():

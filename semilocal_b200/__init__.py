@@ -11,7 +11,8 @@ from ._lib import (ALGO_AUTO, ALGO_HYBRID, ALGO_WAVEFRONT, PLAN_BITPARALLEL, Q_G
                    Q_STRING_SUBSTRING, Q_SUBSTRING_STRING, Q_SUFFIX_PREFIX, SlcsError, lib)
 from .api import (BatchPlan, PairPlan, Server, SteadyAntPlan, Permutation, autotune, set_tuning, tuning, batch_comb, concat_pairs, bitcomb_llcs, comb, lcs, scores, staggered_glue, steady_ant, window_scores, check_permutation, duplicate_search)
 from .strategies import (BitParallelLCS, BraidMultiplicationStrategy, GpuHybridCombing, GpuIterativeCombing,
-                         GpuSteadyAntMultiplication, LCSBySemiLocal, LCSStrategy, SemiLocalStrategy,
+                         GpuSteadyAntMultiplication, InteractiveDuplicateSearchSemiDense,
+                         InteractiveDuplicateSearchSemiSparse, LCSBySemiLocal, LCSStrategy, SemiLocalStrategy,
                          StaggeredStickyBraidMultiplication)
 
 __all__ = [
@@ -19,5 +20,6 @@ __all__ = [
     "Q_SUBSTRING_STRING", "Q_SUFFIX_PREFIX", "SlcsError", "lib", "BatchPlan", "PairPlan", "Server", "autotune", "set_tuning", "tuning", "SteadyAntPlan", "concat_pairs", "Permutation", "batch_comb", "bitcomb_llcs",
     "comb", "lcs", "scores", "staggered_glue", "steady_ant", "window_scores", "check_permutation", "duplicate_search", "BitParallelLCS", "BraidMultiplicationStrategy",
     "GpuHybridCombing", "GpuIterativeCombing", "GpuSteadyAntMultiplication", "LCSBySemiLocal", "LCSStrategy",
-    "SemiLocalStrategy", "StaggeredStickyBraidMultiplication",
+    "SemiLocalStrategy", "StaggeredStickyBraidMultiplication", "InteractiveDuplicateSearchSemiDense",
+    "InteractiveDuplicateSearchSemiSparse",
 ]

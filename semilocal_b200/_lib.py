@@ -126,6 +126,10 @@ SIGNATURES = {
     "slcs_window_scores_dev": [_vp, _vp, _int, _int, _int, _vp, _vp],
     "slcs_duplicate_search_u8": [_u8p, _int, _u8p, _int, ctypes.c_double, ctypes.POINTER(Interval), _int, _i32p],
     "slcs_duplicate_search_i32": [_i32p, _int, _i32p, _int, ctypes.c_double, ctypes.POINTER(Interval), _int, _i32p],
+    "slcs_duplicate_search_sparse_u8": [_u8p, _int, _u8p, _int, ctypes.c_double, ctypes.POINTER(Interval), _int,
+                                        _i32p],
+    "slcs_duplicate_search_sparse_i32": [_i32p, _int, _i32p, _int, ctypes.c_double, ctypes.POINTER(Interval), _int,
+                                         _i32p],
     "slcs_server_window": [_vp, ctypes.c_uint64, _int, _i32p],
     "slcs_selftest_wait_timeout": [_i32p],
     "slcs_check_permutation": [_i32p, _int, _i32p],

@@ -145,17 +145,19 @@ def window_scores(row_to_col, m: int, n: int, w: int) -> np.ndarray:
     return out[:max(n - w + 1, 0)]
 
 
-def duplicate_search(pattern, text, k: float) -> List[Tuple[int, int, float]]:
+def duplicate_search(pattern, text, k: float, sparse: bool = False) -> List[Tuple[int, int, float]]:
     """Approximate copies of `pattern` in `text` as (start, end, score) intervals: the result vector of the
-    reference's InteractiveDuplicateSearchSemiDense::find (R:approximate_matching/ApproximateMatching.h:320-420)
-    for the same symbols and k (0 < k <= 1), computed from one braid on the device."""
+    reference's InteractiveDuplicateSearchSemiDense::find (sparse=False) or ...SemiSparse::find (sparse=True)
+    (R:approximate_matching/ApproximateMatching.h:252-420) for the same symbols and k (0 < k <= 1), computed from
+    one braid on the device."""
     p = np.asarray(pattern)
     t = np.asarray(text)
+    suffix = "sparse_" if sparse else ""
     if p.dtype == np.uint8 and t.dtype == np.uint8:
-        fn, ptr = lib().slcs_duplicate_search_u8, _u8p
+        fn, ptr = getattr(lib(), f"slcs_duplicate_search_{suffix}u8"), _u8p
     else:
         p, t = p.astype(np.int32), t.astype(np.int32)
-        fn, ptr = lib().slcs_duplicate_search_i32, _i32p
+        fn, ptr = getattr(lib(), f"slcs_duplicate_search_{suffix}i32"), _i32p
     p, t = np.ascontiguousarray(p), np.ascontiguousarray(t)
     cap = max(len(t) - int(len(p) / k) + 2, 1) if k > 0 else 1
     out = (_lib.Interval * cap)()

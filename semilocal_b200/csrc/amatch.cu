@@ -46,11 +46,22 @@ __device__ __forceinline__ long long warp_max64(long long v) {
     return v;
 }
 
+// W(i) of a start whose window reaches the threshold joins the candidate list (unordered: (i, start, end, score))
+__device__ __forceinline__ void am_emit(const int32_t *wlcs, int m, int w, double kdi, int i, long long b,
+                                        int *ncand, int4 *cand, int cap) {
+    if (2.0 * wlcs[i] - m - w < kdi) return;   // the window's own score, as the reference computes it
+    const int rel = static_cast<int>(b & ((1 << kAmBits) - 1));
+    const int len = static_cast<int>((b >> kAmBits) & ((1 << kAmBits) - 1));
+    const int pos = atomicAdd(ncand, 1);
+    if (pos < cap) cand[pos] = make_int4(i, i + rel - len, i + rel, static_cast<int>(b >> (2 * kAmBits)));
+}
+
 // One warp per chunk of `chunk` window starts.  Shared memory: D, best start and best score of every end, indexed
-// by end mod S.  out[i] = (start, end, score) of W(i).
+// by end mod S.  Candidates (see am_emit) go to cand[0 .. *ncand).
 __global__ void __launch_bounds__(32) am_window_kernel(const int32_t *__restrict__ r2c, const int32_t *__restrict__ c2r,
                                                        const int32_t *__restrict__ wlcs, int m, int n, int w, int L,
-                                                       int chunk, int4 *__restrict__ out) {
+                                                       int chunk, double kdi, int *__restrict__ ncand,
+                                                       int4 *__restrict__ cand, int cap) {
     extern __shared__ int am_smem[];
     const int S = w - L + 1;
     int *D = am_smem, *bs = am_smem + S, *bsc = am_smem + 2 * S;
@@ -97,11 +108,7 @@ __global__ void __launch_bounds__(32) am_window_kernel(const int32_t *__restrict
     }
     if (i_top <= i_hi) {
         const long long b = warp_max64(best);
-        if (lane == 0) {
-            const int rel = static_cast<int>(b & ((1 << kAmBits) - 1));
-            const int len = static_cast<int>((b >> kAmBits) & ((1 << kAmBits) - 1));
-            out[i_top] = make_int4(i_top + rel - len, i_top + rel, static_cast<int>(b >> (2 * kAmBits)), 0);
-        }
+        if (lane == 0) am_emit(wlcs, m, w, kdi, i_top, b, ncand, cand, cap);
     }
     __syncwarp();
     // ---- steps i = i_top - 1 .. i_lo: strand m + i joins, end i + L enters, end i + 1 + w leaves ----
@@ -150,18 +157,18 @@ __global__ void __launch_bounds__(32) am_window_kernel(const int32_t *__restrict
         __syncwarp();
         if (i <= i_hi) {
             const long long b = warp_max64(best);
-            if (lane == 0) {
-                const int rel = static_cast<int>(b & ((1 << kAmBits) - 1));
-                const int len = static_cast<int>((b >> kAmBits) & ((1 << kAmBits) - 1));
-                out[i] = make_int4(i + rel - len, i + rel, static_cast<int>(b >> (2 * kAmBits)), 0);
-            }
+            if (lane == 0) am_emit(wlcs, m, w, kdi, i, b, ncand, cand, cap);
         }
     }
 }
 
+// sparse = false: InteractiveDuplicateSearchSemiDense (every window start, from the end of the text);
+// sparse = true: InteractiveDuplicateSearchSemiSparse (R:approximate_matching/ApproximateMatching.h:252-318): the
+// windows its first phase visits (it skips ahead by half the score deficit), each a clone whose best interval is
+// the triangle of the clone's own braid -- the same interval W(start), read here from the one braid of the text.
 template <typename T>
-int duplicate_search(const T *pattern, int m, const T *text, int n, double k, slcs_interval *out, int cap,
-                     int *n_out) {
+int duplicate_search(const T *pattern, int m, const T *text, int n, double k, bool sparse, slcs_interval *out,
+                     int cap, int *n_out) {
     if (!n_out || m <= 0 || n <= 0 || !pattern || !text || cap < 0 || (cap > 0 && !out))
         return fail(SLCS_ERR_ARG, "bad arguments");
     if (!(k > 0.0 && k <= 1.0)) return fail(SLCS_ERR_ARG, "k must lie in (0, 1]");
@@ -181,13 +188,15 @@ int duplicate_search(const T *pattern, int m, const T *text, int n, double k, sl
     const int nstart = n - w + 1;
     DevBuf<T> dp, dt;
     DevBuf<int32_t> r2c, c2r, wl;
-    DevBuf<int4> dw;
+    DevBuf<int4> dc;
+    DevBuf<int> dn;
     SLCS_TRY(dp.alloc(m, s));
     SLCS_TRY(dt.alloc(n, s));
     SLCS_TRY(r2c.alloc(m + n, s));
     SLCS_TRY(c2r.alloc(m + n, s));
     SLCS_TRY(wl.alloc(nstart, s));
-    SLCS_TRY(dw.alloc(nstart, s));
+    SLCS_TRY(dn.alloc(1, s));
+    SLCS_CUDA_TRY(cudaMemsetAsync(dn.p, 0, sizeof(int), s));
     SLCS_CUDA_TRY(cudaMemcpyAsync(dp.p, pattern, sizeof(T) * m, cudaMemcpyHostToDevice, s));
     SLCS_CUDA_TRY(cudaMemcpyAsync(dt.p, text, sizeof(T) * n, cudaMemcpyHostToDevice, s));
     // a short pattern against a long text: one row of tiles, glued on the pattern's m strands
@@ -201,13 +210,27 @@ int duplicate_search(const T *pattern, int m, const T *text, int n, double k, sl
     const size_t smem = sizeof(int) * 3 * (size_t) S;
     if (smem > 48 * 1024)
         SLCS_CUDA_TRY(cudaFuncSetAttribute(am_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    am_window_kernel<<<(nstart + chunk - 1) / chunk, 32, smem, s>>>(r2c.p, c2r.p, wl.p, m, n, w, L, chunk, dw.p);
-    SLCS_CUDA_TRY(cudaGetLastError());
-    std::vector<int4> W(nstart);
-    std::vector<int32_t> lcs(nstart);
-    SLCS_CUDA_TRY(cudaMemcpyAsync(W.data(), dw.p, sizeof(int4) * nstart, cudaMemcpyDeviceToHost, s));
-    SLCS_CUDA_TRY(cudaMemcpyAsync(lcs.data(), wl.p, sizeof(int32_t) * nstart, cudaMemcpyDeviceToHost, s));
+    // candidate list: sized for the usual case, grown and rerun in the rare case of more windows over the bar
+    int capc = std::min(nstart, 1 << 16), ncand = 0;
+    std::vector<int4> C;
+    for (;;) {
+        SLCS_TRY(dc.alloc(capc, s));
+        am_window_kernel<<<(nstart + chunk - 1) / chunk, 32, smem, s>>>(r2c.p, c2r.p, wl.p, m, n, w, L, chunk, kdi,
+                                                                        dn.p, dc.p, capc);
+        SLCS_CUDA_TRY(cudaGetLastError());
+        SLCS_CUDA_TRY(cudaMemcpyAsync(&ncand, dn.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        SLCS_CUDA_TRY(cudaStreamSynchronize(s));
+        if (ncand <= capc) break;
+        capc = ncand;
+        dc.release();
+        SLCS_CUDA_TRY(cudaMemsetAsync(dn.p, 0, sizeof(int), s));
+    }
+    C.resize(ncand);
+    if (ncand) SLCS_CUDA_TRY(cudaMemcpyAsync(C.data(), dc.p, sizeof(int4) * ncand, cudaMemcpyDeviceToHost, s));
+    std::vector<int32_t> lcs(sparse ? nstart : 0);   // the sparse walk reads every visited window's score
+    if (sparse) SLCS_CUDA_TRY(cudaMemcpyAsync(lcs.data(), wl.p, sizeof(int32_t) * nstart, cudaMemcpyDeviceToHost, s));
     SLCS_CUDA_TRY(cudaStreamSynchronize(s));
+    std::sort(C.begin(), C.end(), [](const int4 &x, const int4 &y) { return x.x < y.x; });   // by window start
     // candidates in the reference's order (starts from n - w down), distinct by (start, end)
     struct Iv {
         int start, end;
@@ -215,13 +238,28 @@ int duplicate_search(const T *pattern, int m, const T *text, int n, double k, sl
     };
     std::vector<Iv> cand;
     std::unordered_set<long long> seen;
-    for (int i = nstart - 1; i >= 0; --i) {
-        const double wdist = 2.0 * lcs[i] - m - w;   // score(i, i + w)
-        if (wdist < kdi) continue;
-        const long long key = (static_cast<long long>(W[i].x) << 32) | static_cast<unsigned>(W[i].y);
-        if (seen.insert(key).second) cand.push_back(Iv{W[i].x, W[i].y, static_cast<double>(W[i].z)});
+    auto take = [&](const int4 &c) {
+        const long long key = (static_cast<long long>(c.y) << 32) | static_cast<unsigned>(c.z);
+        if (seen.insert(key).second) cand.push_back(Iv{c.y, c.z, static_cast<double>(c.w)});
+    };
+    if (!sparse) {
+        for (int q = ncand - 1; q >= 0; --q) take(C[q]);   // starts from n - w down
+        std::reverse(cand.begin(), cand.end());
+    } else {
+        // the first phase's walk over window ends (ApproximateMatching.h:261-272); a visited window over the bar
+        // is one of the candidates of the list
+        for (int end = w; end < n + 1;) {
+            const double dist = 2.0 * lcs[end - w] - m - w;
+            if (dist >= kdi) {
+                const auto it = std::lower_bound(C.begin(), C.end(), end - w,
+                                                 [](const int4 &c, int i) { return c.x < i; });
+                if (it == C.end() || it->x != end - w) return fail(SLCS_ERR_INTERNAL, "window missing from the list");
+                take(*it);
+            }
+            if (dist < kdi - 1) end += std::max(1, int((std::abs(dist) - std::abs(kdi)) / 2));
+            else ++end;
+        }
     }
-    std::reverse(cand.begin(), cand.end());
     // the greedy pick (R:approximate_matching/ApproximateMatching.h:186-200)
     std::sort(cand.begin(), cand.end(), [](const Iv &a, const Iv &b) {
         return (a.start < b.start) || (a.start == b.start && a.score > b.score);
@@ -248,12 +286,22 @@ extern "C" {
 
 int slcs_duplicate_search_u8(const uint8_t *pattern, int m, const uint8_t *text, int n, double k, slcs_interval *out,
                              int out_cap, int *n_out) {
-    return duplicate_search<uint8_t>(pattern, m, text, n, k, out, out_cap, n_out);
+    return duplicate_search<uint8_t>(pattern, m, text, n, k, false, out, out_cap, n_out);
 }
 
 int slcs_duplicate_search_i32(const int32_t *pattern, int m, const int32_t *text, int n, double k,
                               slcs_interval *out, int out_cap, int *n_out) {
-    return duplicate_search<int32_t>(pattern, m, text, n, k, out, out_cap, n_out);
+    return duplicate_search<int32_t>(pattern, m, text, n, k, false, out, out_cap, n_out);
+}
+
+int slcs_duplicate_search_sparse_u8(const uint8_t *pattern, int m, const uint8_t *text, int n, double k,
+                                    slcs_interval *out, int out_cap, int *n_out) {
+    return duplicate_search<uint8_t>(pattern, m, text, n, k, true, out, out_cap, n_out);
+}
+
+int slcs_duplicate_search_sparse_i32(const int32_t *pattern, int m, const int32_t *text, int n, double k,
+                                     slcs_interval *out, int out_cap, int *n_out) {
+    return duplicate_search<int32_t>(pattern, m, text, n, k, true, out, out_cap, n_out);
 }
 
 }  // extern "C"

@@ -126,9 +126,11 @@ struct DevBuf {
         count = cnt;
         return dalloc(reinterpret_cast<void **>(&p), (cnt ? cnt : 1) * sizeof(T), st);
     }
-    ~DevBuf() {
+    void release() {
         if (p) dfree(p, s);
+        p = nullptr;
     }
+    ~DevBuf() { release(); }
 };
 
 // ------------------------------------------------------------------------------------------------

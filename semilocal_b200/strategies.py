@@ -100,3 +100,19 @@ class BitParallelLCS(LCSStrategy):
 
     def compute(self, a, b) -> int:
         return api.bitcomb_llcs(a, b)
+
+
+class InteractiveDuplicateSearchSemiDense:
+    """InteractiveDuplicateSearchSemiDense::find (R:approximate_matching/ApproximateMatching.h:320-420): appends the
+    (start, end, score) intervals the reference finds to `result`."""
+
+    sparse = False
+
+    def find(self, p, text, k: float, result: list) -> None:
+        result.extend(api.duplicate_search(p, text, k, sparse=self.sparse))
+
+
+class InteractiveDuplicateSearchSemiSparse(InteractiveDuplicateSearchSemiDense):
+    """InteractiveDuplicateSearchSemiSparse::find (R:approximate_matching/ApproximateMatching.h:252-318)."""
+
+    sparse = True

@@ -4,7 +4,8 @@
 //
 //   stdin: m n, a[0..m), b[0..n), k, p[0..k), q[0..k)
 //   stdout: one line per result: "comb <r2c...>", "hybrid <r2c...>", "score <s>", "lcs <s>", "bit <s>",
-//           "sa <r...>", "glue <r2c...>", "queries <q...>"; or "error <code> <message>"
+//           "sa <r...>", "glue <r2c...>", "queries <q...>", "dup <start end score ...>"; or "error <code> <message>"
+#include <algorithm>
 #include <iostream>
 #include <vector>
 
@@ -52,6 +53,16 @@ int main() {
         slcs::GpuIterativeCombing<int>().compute(a.data() + h, m - h, b.data(), n, bot);
         slcs::GpuStaggeredGlue<>().glue(top, bot, true, whole);
         print("glue", slcs::row_to_col_of(whole));
+        // approximate copies of a's first 40 symbols in b (InteractiveDuplicateSearchSemiDense::find's shape)
+        std::vector<slcs::Interval> dup;
+        slcs::GpuDuplicateSearchSemiDense().find(a.data(), std::min(m, 40), b.data(), n, 0.8, dup);
+        std::vector<long> flat;
+        for (const auto &iv : dup) {
+            flat.push_back(iv.start);
+            flat.push_back(iv.end);
+            flat.push_back(static_cast<long>(iv.score));
+        }
+        print("dup", flat);
     } catch (const slcs::Error &e) {
         std::cout << "error " << e.code() << ' ' << e.what() << '\n';
         return 3;

@@ -1,5 +1,6 @@
-"""Generate tests/golden/amatch_golden.json: the result of the reference's own approximate pattern search,
-InteractiveDuplicateSearchSemiDense::find (R:approximate_matching/ApproximateMatching.h:320-420, compiled from the
+"""Generate tests/golden/amatch_golden.json: the results of the reference's own approximate pattern search,
+InteractiveDuplicateSearchSemiDense::find and ...SemiSparse::find (R:approximate_matching/ApproximateMatching.h:
+252-420, compiled from the
 reference sources into oracle/_ref/libslcs_ref_am.so by oracle/build_ref.sh), on seeded inputs with planted
 copies (semilocal_b200.gen.planted_text).  Run where the reference is present:
 
@@ -27,11 +28,13 @@ def main():
     for m, n, copies, alpha, seed, k in CASES:
         p, t = gen.planted_text(m, n, copies, alpha, seed)
         res = O.ref_duplicate_search(p, t, k)
+        sp = O.ref_duplicate_search(p, t, k, kind="sparse")
         out.append({"m": m, "n": n, "copies": copies, "alphabet": alpha, "seed": seed, "k": k,
-                    "intervals": [[s, e, sc] for s, e, sc in res]})
+                    "intervals": [[s, e, sc] for s, e, sc in res],
+                    "intervals_sparse": [[s, e, sc] for s, e, sc in sp]})
     path = os.path.join(ROOT, "tests", "golden", "amatch_golden.json")
     with open(path, "w") as f:
-        json.dump({"source": "InteractiveDuplicateSearchSemiDense::find of the reference, int symbols", "cases": out}, f)
+        json.dump({"source": "InteractiveDuplicateSearchSemiDense / SemiSparse::find of the reference, int symbols", "cases": out}, f)
     print(path, sum(len(c["intervals"]) for c in out), "intervals")
 
 

@@ -1,5 +1,5 @@
-"""Approximate pattern search on the host: the oracle's restatement of InteractiveDuplicateSearchSemiDense
-(oracle/amatch_oracle.cpp) against the reference's own result vectors (tests/golden/amatch_golden.json, made by the
+"""Approximate pattern search on the host: the oracle's restatements of InteractiveDuplicateSearchSemiDense and
+...SemiSparse (oracle/amatch_oracle.cpp) against the reference's own result vectors (tests/golden/amatch_golden.json, made by the
 reference compiled from its sources) and, where that library is present, against the reference on seeded inputs."""
 import json
 import os
@@ -17,23 +17,25 @@ def golden_cases():
     return json.load(open(GOLDEN))["cases"]
 
 
-def test_oracle_matches_golden():
+@pytest.mark.parametrize("sparse", [False, True])
+def test_oracle_matches_golden(sparse):
     for c in golden_cases():
         p, t = gen.planted_text(c["m"], c["n"], c["copies"], c["alphabet"], c["seed"])
-        got = O.duplicate_search(p, t, c["k"])
-        assert [list(x) for x in got] == c["intervals"], (c["m"], c["n"], c["k"])
+        got = O.duplicate_search(p, t, c["k"], sparse=sparse)
+        assert [list(x) for x in got] == c["intervals_sparse" if sparse else "intervals"], (c["m"], c["n"], c["k"])
 
 
-def test_oracle_matches_reference():
+@pytest.mark.parametrize("sparse", [False, True])
+def test_oracle_matches_reference(sparse):
     if O.ref_am() is None:
         pytest.skip("reference library not built here")
-    rng = np.random.default_rng(11)
-    for trial in range(120):
+    rng = np.random.default_rng(11 + sparse)
+    for trial in range(80):
         m = int(rng.integers(1, 60))
         k = float(rng.choice([0.5, 0.7, 0.8, 0.9, 1.0, rng.uniform(0.3, 1.0)]))
         n = int(rng.integers(int(m / k), int(m / k) + 800))
         p, t = gen.planted_text(m, n, int(rng.integers(0, 8)), int(rng.choice([2, 4])), 500 + trial)
-        assert O.duplicate_search(p, t, k) == O.ref_duplicate_search(p, t, k), (m, n, k)
+        assert O.duplicate_search(p, t, k, sparse) == O.ref_duplicate_search(p, t, k, "sparse" if sparse else "dense")
 
 
 def test_oracle_rejects_bad_arguments():

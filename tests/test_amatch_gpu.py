@@ -1,5 +1,5 @@
-"""Approximate pattern search on the GPU (slcs_duplicate_search_*): the result vector of the reference's
-InteractiveDuplicateSearchSemiDense::find, bit for bit, against the reference's own golden results and the
+"""Approximate pattern search on the GPU (slcs_duplicate_search_*): the result vectors of the reference's
+InteractiveDuplicateSearchSemiDense::find and ...SemiSparse::find, bit for bit, against the reference's own golden results and the
 oracle's restatement, through the C ABI."""
 import json
 import os
@@ -14,11 +14,22 @@ pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "amatch_golden.json")
 
 
-def test_golden(engine):
+@pytest.mark.parametrize("sparse", [False, True])
+def test_golden(engine, sparse):
     for c in json.load(open(GOLDEN))["cases"]:
         p, t = gen.planted_text(c["m"], c["n"], c["copies"], c["alphabet"], c["seed"])
-        got = engine.duplicate_search(p, t, c["k"])
-        assert [list(x) for x in got] == c["intervals"], (c["m"], c["n"], c["k"])
+        got = engine.duplicate_search(p, t, c["k"], sparse=sparse)
+        assert [list(x) for x in got] == c["intervals_sparse" if sparse else "intervals"], (c["m"], c["n"], c["k"])
+
+
+def test_sparse_random_vs_oracle(engine, oracle):
+    rng = np.random.default_rng(9)
+    for trial in range(25):
+        m = int(rng.integers(1, 120))
+        k = float(rng.choice([0.5, 0.75, 0.9, 1.0, rng.uniform(0.3, 1.0)]))
+        n = int(rng.integers(int(m / k), int(m / k) + 6000))
+        p, t = gen.planted_text(m, n, int(rng.integers(0, 30)), int(rng.choice([2, 4])), 1900 + trial)
+        assert engine.duplicate_search(p, t, k, sparse=True) == oracle.duplicate_search(p, t, k, sparse=True), (m, n, k)
 
 
 @pytest.mark.parametrize("symbols", ["u8", "i32"])

@@ -59,6 +59,8 @@ def test_adapter_matches_oracle(engine, tmp_path):
     assert out["queries"] == [score, O.lcs_dp(a, b[n // 4:n // 2]), O.lcs_dp(a[:m // 3], b[n // 5:])]
     assert np.array_equal(out["sa"], O.steady_ant(p, q))
     assert np.array_equal(out["glue"], braid)
+    dup = O.duplicate_search(a[:40], b, 0.8)
+    assert len(dup) > 0 and out["dup"] == [int(v) for iv in dup for v in iv]
 
 
 @pytest.mark.gpu
