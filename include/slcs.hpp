@@ -24,6 +24,7 @@
 #include <stdexcept>
 #include <string>
 #include <type_traits>
+#include <algorithm>
 #include <vector>
 
 #include "slcs.h"
@@ -225,12 +226,18 @@ public:
     template <class T>
     void find(const T *p, int p_size, const T *text, int text_size, double k, std::vector<Interval> &result) const {
         std::vector<int32_t> pp(p, p + p_size), tt(text, text + text_size);
-        const int cap = text_size + 1;
-        std::vector<slcs_interval> out(cap);
+        int cap = text_size / std::max(int(p_size * k), 1) + 2;   // picked intervals: disjoint, >= int(m k) long
+        std::vector<slcs_interval> out;
         int cnt = 0;
-        check(Sparse ? slcs_duplicate_search_sparse_i32(pp.data(), p_size, tt.data(), text_size, k, out.data(), cap, &cnt)
-                     : slcs_duplicate_search_i32(pp.data(), p_size, tt.data(), text_size, k, out.data(), cap, &cnt));
-        for (int i = 0; i < cnt && i < cap; ++i) result.push_back(Interval{out[i].start, out[i].end, out[i].score});
+        for (;;) {
+            out.resize(cap);
+            check(Sparse ? slcs_duplicate_search_sparse_i32(pp.data(), p_size, tt.data(), text_size, k, out.data(), cap,
+                                                            &cnt)
+                         : slcs_duplicate_search_i32(pp.data(), p_size, tt.data(), text_size, k, out.data(), cap, &cnt));
+            if (cnt <= cap) break;
+            cap = cnt;
+        }
+        for (int i = 0; i < cnt; ++i) result.push_back(Interval{out[i].start, out[i].end, out[i].score});
     }
 };
 using GpuDuplicateSearchSemiDense = GpuDuplicateSearch<false>;

@@ -159,11 +159,15 @@ def duplicate_search(pattern, text, k: float, sparse: bool = False) -> List[Tupl
         p, t = p.astype(np.int32), t.astype(np.int32)
         fn, ptr = getattr(lib(), f"slcs_duplicate_search_{suffix}i32"), _i32p
     p, t = np.ascontiguousarray(p), np.ascontiguousarray(t)
-    cap = max(len(t) - int(len(p) / k) + 2, 1) if k > 0 else 1
-    out = (_lib.Interval * cap)()
-    cnt = ctypes.c_int32(0)
-    check(fn(_p(p, ptr), len(p), _p(t, ptr), len(t), ctypes.c_double(k), out, cap, ctypes.byref(cnt)))
-    return [(out[i].start, out[i].end, out[i].score) for i in range(min(cnt.value, cap))]
+    # the picked intervals do not overlap and are at least int(m k) long
+    cap = len(t) // max(int(len(p) * k), 1) + 2 if k > 0 else 1
+    while True:
+        out = (_lib.Interval * cap)()
+        cnt = ctypes.c_int32(0)
+        check(fn(_p(p, ptr), len(p), _p(t, ptr), len(t), ctypes.c_double(k), out, cap, ctypes.byref(cnt)))
+        if cnt.value <= cap:
+            return [(out[i].start, out[i].end, out[i].score) for i in range(cnt.value)]
+        cap = cnt.value
 
 
 def scores(row_to_col, m: int, n: int, queries: Sequence[Tuple[int, int, int]]) -> np.ndarray:

@@ -126,13 +126,34 @@ int comb_wavefront_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int3
     return check_dev_err(err.p, s);
 }
 
+// The last hybrid plan of each device, kept for the next call of the same shape (planning a hybrid -- tile
+// descriptors, glue levels, steady-ant plans, scratch -- costs far more host time than running a small one).  A
+// call that finds it busy or of another shape plans afresh and then offers its plan in its place.
+struct HybridCache {
+    std::mutex mu;
+    HybridPlan *H = nullptr;
+    int m = -1, n = -1, tr = -1, tc = -1, elem = 0;
+    bool busy = false;
+};
+HybridCache g_hcache[64];
+
 template <typename T>
 int comb_hybrid_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int32_t *d_r2c, int32_t *d_c2r,
                     int32_t *d_score, const slcs_opts *opts, cudaStream_t s) {
     const int tr = (opts && opts->tile_rows > 0) ? opts->tile_rows : pick_tile();
     const int tc = (opts && opts->tile_cols > 0) ? opts->tile_cols : pick_tile();
+    HybridCache &C = g_hcache[E->device];
     HybridPlan *H = nullptr;
-    SLCS_TRY(hybrid_plan_create(m, n, tr, tc, E, s, &H));
+    bool from_cache = false;
+    {
+        std::lock_guard<std::mutex> lk(C.mu);
+        if (!C.busy && C.H && C.m == m && C.n == n && C.tr == tr && C.tc == tc && C.elem == (int) sizeof(T)) {
+            H = C.H;
+            C.busy = true;
+            from_cache = true;
+        }
+    }
+    if (!H) SLCS_TRY(hybrid_plan_create(m, n, tr, tc, E, s, &H));
     DevBuf<int> err;
     int rc = err.alloc(1, s);
     if (rc == SLCS_OK && cudaMemsetAsync(err.p, 0, sizeof(int), s) != cudaSuccess) rc = fail(SLCS_ERR_CUDA, "memset");
@@ -144,8 +165,29 @@ int comb_hybrid_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int32_t
                                                   cudaMemcpyDeviceToDevice, s) != cudaSuccess)
         rc = fail(SLCS_ERR_CUDA, "result copy");
     if (rc == SLCS_OK && d_score) rc = hybrid_score(H, d_score, s);
-    if (rc == SLCS_OK) rc = check_dev_err(err.p, s);
-    hybrid_plan_destroy(H);
+    if (rc == SLCS_OK) rc = check_dev_err(err.p, s);   // the plan's work is over when this returns
+    HybridPlan *drop = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(C.mu);
+        if (from_cache) {
+            C.busy = false;
+            if (rc != SLCS_OK) {   // a failed run leaves no plan behind
+                drop = C.H;
+                C.H = nullptr;
+            }
+        } else if (rc == SLCS_OK && !C.busy) {
+            drop = C.H;
+            C.H = H;
+            C.m = m;
+            C.n = n;
+            C.tr = tr;
+            C.tc = tc;
+            C.elem = (int) sizeof(T);
+        } else {
+            drop = H;
+        }
+    }
+    if (drop) hybrid_plan_destroy(drop);
     return rc;
 }
 
@@ -238,6 +280,18 @@ int slcs_set_device(int device) {
 int slcs_release(void) {
     Engine *E;
     SLCS_TRY(engine(&E));
+    {
+        HybridCache &C = g_hcache[E->device];
+        HybridPlan *drop = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(C.mu);
+            if (!C.busy) {
+                drop = C.H;
+                C.H = nullptr;
+            }
+        }
+        if (drop) hybrid_plan_destroy(drop);
+    }
     SLCS_CUDA_TRY(cudaStreamSynchronize(E->stream));
     cudaMemPool_t pool;
     SLCS_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, E->device));

@@ -4,6 +4,7 @@
     python -m semilocal_b200.profile_cases bit    [log2 n]    # bit-parallel combing (bit_kernel)
     python -m semilocal_b200.profile_cases wave   [log2 n]    # wavefront combing of one pair (comb_kernel)
     python -m semilocal_b200.profile_cases hybrid [log2 n]    # hybrid: tile combing + glue tree
+    python -m semilocal_b200.profile_cases amatch [log2 n]    # approximate search: pattern 1000, planted text
     python -m semilocal_b200.profile_cases sa     [log2 n]    # steady ant (sa_* kernels)
     python -m semilocal_b200.profile_cases probe              # the combing roofline probe (probe_cells_kernel)
 
@@ -75,6 +76,15 @@ def main(argv):
         torch.cuda.synchronize()
         sp.check(sh)
         print(f"sa n=2^{lg} wall_ms={(time.perf_counter() - t0) / 3 * 1e3:.2f} ok={bool(np.array_equal(np.sort(dr.cpu().numpy()), np.arange(1 << lg)))}")
+        return
+    if case == "amatch":
+        lg = arg or 22
+        p, t = gen.planted_text(1000, 1 << lg, 200, 4, 31)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            found = S.duplicate_search(p, t, 0.9)
+        print(f"amatch pattern=1000 text=2^{lg} k=0.9 intervals={len(found)} "
+              f"wall_ms={(time.perf_counter() - t0) / 3 * 1e3:.2f}")
         return
     raise SystemExit(f"unknown case {case}")
 
