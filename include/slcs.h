@@ -80,8 +80,9 @@ int slcs_comb_i32(const int32_t *a, int m, const int32_t *b, int n, int32_t *row
 int slcs_comb_u8_dev(const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_row_to_col,
                      int32_t *d_col_to_row, int32_t *d_score, const slcs_opts *opts, void *stream);
 /* Allocation-free variant of slcs_comb_u8_dev, for callers that cannot let the engine allocate device
- * memory (a host that owns a fixed device-memory budget, code running under a no-allocation policy during
- * graph capture, a serving loop that must not touch the allocator).  No counterpart in the reference.
+ * memory (a host that owns a fixed device-memory budget, a plugin in an application whose allocator
+ * reserved the device memory up front, a serving loop that must not touch the allocator).
+ * No counterpart in the reference.
  * Its scratch is one static device array of about 192 KiB per device (held until the process exits),
  * shared by every call and cleared by each call: calls that overlap on the GPU race, so serialise them.
  * The first call on a device resolves the array's address; make it before any stream capture.

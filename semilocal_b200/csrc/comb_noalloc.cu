@@ -1,9 +1,9 @@
 // comb_noalloc.cu -- an allocation-free entry point for single-pair combing on device memory.
 //
 // Some callers cannot allocate device memory on the engine's behalf: a host that hands the engine a fixed
-// device-memory budget and owns every allocation itself, code that runs while a CUDA graph is being
-// captured under a no-allocation policy, or a latency-bound serving loop that must never touch the
-// allocator (cudaMalloc may synchronise the device and can fail under fragmentation).  For them,
+// device-memory budget and owns every allocation itself, a plugin inside an application whose own
+// allocator reserved the device memory up front, or a latency-bound serving loop that must never touch
+// the allocator (cudaMalloc may synchronise the device and can fail under fragmentation).  For them,
 // slcs_comb_u8_dev_noalloc runs the same wavefront combing as slcs_comb_u8_dev but keeps all of its
 // scratch (band progress counters, work items, the pair descriptor, the dequeue counter and the error
 // word) in one file-scope __device__ array of fixed size, kNoAllocScratchBytes below.  The caller still

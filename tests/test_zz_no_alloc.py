@@ -2,8 +2,8 @@
 point (slcs_comb_u8_dev), called through the C ABI on torch-owned device buffers.
 
 It exists for callers that cannot let the engine allocate device memory (a fixed device-memory budget
-owned by the host, a no-allocation policy while a CUDA graph is captured, a serving loop that must not
-touch the allocator); its scratch is a static device array shared by all calls.  Braids are integers,
+owned by the host, a plugin in an application whose allocator reserved the device memory up front, a
+serving loop that must not touch the allocator); its scratch is a static device array shared by all calls.  Braids are integers,
 so the tolerance is exact equality.  Two calls in a row check that the shared scratch is cleared between
 calls.  This file is collected last so that a run stopping at the first failure has run every other test.
 """
