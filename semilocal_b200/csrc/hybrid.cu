@@ -212,6 +212,12 @@ void hybrid_plan_destroy(HybridPlan *H) {
     delete H;
 }
 
+void hybrid_plan_set_stream(HybridPlan *H, cudaStream_t s) {
+    if (!H) return;
+    H->s = s;
+    for (GlueLevel &L : H->levels) sa_plan_set_stream(L.sa, s);
+}
+
 namespace {
 template <typename T>
 int up(T **dst, const std::vector<T> &v, cudaStream_t s) {

@@ -201,6 +201,8 @@ int sa_plan_run(SaPlan *P, const int32_t *d_P, const int32_t *d_Q, int32_t *d_R,
 int sa_plan_run_ex(SaPlan *P, const int32_t *d_P, const int32_t *d_leafP, const int32_t *d_Q, int32_t *d_R,
                    int32_t *d_PLout, int32_t *d_QLout, int *d_err, cudaStream_t s);
 void sa_plan_destroy(SaPlan *P);
+// The stream the plan's buffers are freed on; only for a plan whose work on its old stream has completed.
+void sa_plan_set_stream(SaPlan *P, cudaStream_t s);
 int sa_plan_launches(const SaPlan *P);
 int64_t sa_plan_total(const SaPlan *P);
 
@@ -212,6 +214,10 @@ int hybrid_plan_create(int m, int n, int tile_rows, int tile_cols, Engine *E, cu
 template <typename T>
 int hybrid_plan_run(HybridPlan *H, const T *d_a, const T *d_b, int *d_err, cudaStream_t s);
 void hybrid_plan_destroy(HybridPlan *H);
+// Moves the plan (and its steady-ant plans) onto stream s for its later frees; only once the work queued on the
+// stream it was created on has completed.  A plan that outlives the call that made it is moved onto the engine's
+// own stream, since the caller's stream may be destroyed before the plan is.
+void hybrid_plan_set_stream(HybridPlan *H, cudaStream_t s);
 int32_t *hybrid_result_r2c(HybridPlan *H);
 int32_t *hybrid_result_c2r(HybridPlan *H);
 int hybrid_score(HybridPlan *H, int32_t *d_score, cudaStream_t s);

@@ -1377,6 +1377,10 @@ void sa_plan_destroy(SaPlan *P) {
     delete P;
 }
 
+void sa_plan_set_stream(SaPlan *P, cudaStream_t s) {
+    if (P) P->alloc_stream = s;
+}
+
 // Plans the batched unit-Monge products of problems i = 0..np-1, problem i occupying [off[i], off[i] + n[i])
 // of concatenated row->col arrays.  All task lists and scratch are built and allocated here.
 int sa_plan_create(const std::vector<int64_t> &off, const std::vector<int> &n, SaPlan **out, cudaStream_t s,

@@ -58,3 +58,42 @@ def test_hybrid_equals_wavefront_mutated_pair(engine):
     w, sw = engine.comb(a, b, algo=engine.ALGO_WAVEFRONT)
     assert np.array_equal(h, w) and sh == sw
     assert np.array_equal(np.sort(h), np.arange(len(a) + len(b)))
+
+
+def test_cached_plan_outlives_the_callers_stream(engine, oracle):
+    """The last hybrid plan of a device is kept for the next call of its shape.  It is made on the caller's
+    stream, which the caller may destroy before the plan is replaced: replacing and freeing it afterwards must not
+    touch that stream, and every result stays exact."""
+    import ctypes
+
+    import torch
+    from cuda.bindings import runtime as rt
+
+    S = engine
+    rng = np.random.default_rng(33)
+    first = (_rand(rng, 3000, 4), _rand(rng, 2500, 4))
+    second = (_rand(rng, 1700, 4), _rand(rng, 3900, 4))
+
+    def run(a, b, stream_handle):
+        m, n = len(a), len(b)
+        da = torch.from_numpy(a).cuda()
+        db = torch.from_numpy(b).cuda()
+        r2c = torch.full((m + n,), -1, dtype=torch.int32, device="cuda")
+        o = S._lib.opts(S.ALGO_HYBRID, tile_rows=512, tile_cols=512)
+        torch.cuda.synchronize()
+        S._lib.check(S.lib().slcs_comb_u8_dev(da.data_ptr(), m, db.data_ptr(), n, r2c.data_ptr(), None, None,
+                                              ctypes.byref(o), ctypes.c_void_p(stream_handle)))
+        torch.cuda.synchronize()
+        return r2c.cpu().numpy()
+
+    err, st = rt.cudaStreamCreateWithFlags(rt.cudaStreamNonBlocking)
+    assert err == rt.cudaError_t.cudaSuccess
+    got = [run(*first, int(st))]                    # planned on the caller's stream and kept
+    assert rt.cudaStreamDestroy(st)[0] == rt.cudaError_t.cudaSuccess
+    got.append(run(*first, 0))                      # the kept plan, reused on another stream
+    got.append(run(*second, 0))                     # another shape: the kept plan is replaced and freed
+    got.append(run(*first, 0))                      # the first shape planned afresh
+    exp = [oracle.comb_antidiag(*first, 4), oracle.comb_antidiag(*first, 4), oracle.comb_antidiag(*second, 4),
+           oracle.comb_antidiag(*first, 4)]
+    for k, (g, e) in enumerate(zip(got, exp)):
+        assert np.array_equal(g, e), k
