@@ -20,13 +20,14 @@
 // chunk (S = w - L + 1 ends per window) so that every end's maximum is complete when the chunk begins.  Per end it
 // keeps D(i, r) (one more strand per step: + [row_to_col[m + i] < r]; a new end from its neighbour:
 // D(i, r) = D(i, r + 1) - [col_to_row[r] >= m + i]) and the best interval.  The candidates, their dedup, the sort
-// and the greedy pick run on the host, with the same sort as the reference so that equal keys land alike.
+// and the greedy pick run on the host (amatch_pick.h), with the same sort as the reference so that equal keys land
+// alike.
 #include <algorithm>
 #include <climits>
 #include <cmath>
-#include <unordered_set>
 #include <vector>
 
+#include "amatch_pick.h"
 #include "slcs_internal.cuh"
 
 namespace slcs {
@@ -212,7 +213,7 @@ int duplicate_search(const T *pattern, int m, const T *text, int n, double k, bo
         SLCS_CUDA_TRY(cudaFuncSetAttribute(am_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     // candidate list: sized for the usual case, grown and rerun in the rare case of more windows over the bar
     int capc = std::min(nstart, 1 << 16), ncand = 0;
-    std::vector<int4> C;
+    std::vector<am::Cand> C;
     for (;;) {
         SLCS_TRY(dc.alloc(capc, s));
         am_window_kernel<<<(nstart + chunk - 1) / chunk, 32, smem, s>>>(r2c.p, c2r.p, wl.p, m, n, w, L, chunk, kdi,
@@ -230,49 +231,15 @@ int duplicate_search(const T *pattern, int m, const T *text, int n, double k, bo
     std::vector<int32_t> lcs(sparse ? nstart : 0);   // the sparse walk reads every visited window's score
     if (sparse) SLCS_CUDA_TRY(cudaMemcpyAsync(lcs.data(), wl.p, sizeof(int32_t) * nstart, cudaMemcpyDeviceToHost, s));
     SLCS_CUDA_TRY(cudaStreamSynchronize(s));
-    std::sort(C.begin(), C.end(), [](const int4 &x, const int4 &y) { return x.x < y.x; });   // by window start
-    // candidates in the reference's order (starts from n - w down), distinct by (start, end)
-    struct Iv {
-        int start, end;
-        double score;
-    };
-    std::vector<Iv> cand;
-    std::unordered_set<long long> seen;
-    auto take = [&](const int4 &c) {
-        const long long key = (static_cast<long long>(c.y) << 32) | static_cast<unsigned>(c.z);
-        if (seen.insert(key).second) cand.push_back(Iv{c.y, c.z, static_cast<double>(c.w)});
-    };
-    if (!sparse) {
-        for (int q = ncand - 1; q >= 0; --q) take(C[q]);   // starts from n - w down
-        std::reverse(cand.begin(), cand.end());
-    } else {
-        // the first phase's walk over window ends (ApproximateMatching.h:261-272); a visited window over the bar
-        // is one of the candidates of the list
-        for (int end = w; end < n + 1;) {
-            const double dist = 2.0 * lcs[end - w] - m - w;
-            if (dist >= kdi) {
-                const auto it = std::lower_bound(C.begin(), C.end(), end - w,
-                                                 [](const int4 &c, int i) { return c.x < i; });
-                if (it == C.end() || it->x != end - w) return fail(SLCS_ERR_INTERNAL, "window missing from the list");
-                take(*it);
-            }
-            if (dist < kdi - 1) end += std::max(1, int((std::abs(dist) - std::abs(kdi)) / 2));
-            else ++end;
-        }
-    }
-    // the greedy pick (R:approximate_matching/ApproximateMatching.h:186-200)
-    std::sort(cand.begin(), cand.end(), [](const Iv &a, const Iv &b) {
-        return (a.start < b.start) || (a.start == b.start && a.score > b.score);
-    });
-    int left = 0, right = 0, cnt = 0;
-    for (const Iv &c : cand) {
-        if (c.start > left && c.start >= right) {
-            if (cnt < cap) out[cnt] = slcs_interval{c.start, c.end, c.score};
-            ++cnt;
-            left = c.start;
-            right = std::max(right, c.end);
-        }
-    }
+    // candidates in the reference's order (dense: starts from n - w down; sparse: its first-phase walk), distinct by
+    // (start, end), then the reference's sort and greedy pick
+    am::sort_by_window(C);
+    std::vector<am::Iv> cand;
+    if (!sparse) cand = am::dense_candidates(C);
+    else if (!am::sparse_candidates(C, lcs.data(), m, n, w, kdi, &cand))
+        return fail(SLCS_ERR_INTERNAL, "window missing from the list");
+    const int cnt =
+        am::greedy_pick(cand, cap, [&](int k, const am::Iv &c) { out[k] = slcs_interval{c.start, c.end, c.score}; });
     *n_out = cnt;
     return SLCS_OK;
 }

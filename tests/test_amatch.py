@@ -45,3 +45,17 @@ def test_oracle_rejects_bad_arguments():
             O.duplicate_search(p, t, k)
     with pytest.raises(ValueError):
         O.duplicate_search(p, t[:11], 0.5)   # text shorter than the window int(m / k) = 20
+
+
+def test_host_pick_steps_match_plain_restatement(tmp_path):
+    """The search's host steps after the device (order by window start, distinct intervals, sort, greedy pick:
+    semilocal_b200/csrc/amatch_pick.h) against a plain restatement of the reference's steps on random candidate
+    sets (tests/cpp/amatch_pick_check.cpp)."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "amatch_pick_check")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror", "-I",
+                    os.path.join(root, "semilocal_b200", "csrc"), os.path.join(root, "tests", "cpp", "amatch_pick_check.cpp"),
+                    "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout + r.stderr
