@@ -110,3 +110,34 @@ def test_oracle_against_golden(oracle):
     for k in range(int(g["bit_count"])):
         a, b = g[f"bit{k}_a"], g[f"bit{k}_b"]
         assert oracle.bit_llcs_nary(a, b, 2) == int(g[f"bit{k}_score"]), k
+
+
+@ref_only
+def test_reference_test_grids(oracle):
+    """The oracle against the reference on the grids of the reference's own GoogleTest comparators (sizes, steps
+    and alphabets as there; strings and permutations seeded here): SemiLocalLCSTest.cpp:47-55 (Dummy vs Simple,
+    5..49 squared, 5 letters) and :57-68 (Simple vs OpenMP, 4900..4999 step 11, 11 letters), SteadyAntTest.cpp:
+    43-56 (Naive vs SimpleSticky, 100..299, every 3rd size here) and :59-67 (SimpleSticky vs MemoryOptimized, 1000..29999 step 111),
+    LCSTest.cpp:65-86 (Dummy vs SemiLocal vs SequentialMem, 5..499 with 15 letters; every 7th size pair here)."""
+    rng = np.random.default_rng(50)
+    for m in range(5, 50):
+        for n in range(5, 50):
+            a, b = _rand(rng, m, 5), _rand(rng, n, 5)
+            x = oracle.comb_rowmajor(a, b)
+            assert np.array_equal(x, oracle.ref_comb(a, b, "dummy")), (m, n)
+            assert np.array_equal(x, oracle.ref_comb(a, b, "simple")), (m, n)
+    for m in range(4900, 5000, 11):
+        for n in range(4900, 5000, 33):
+            a, b = _rand(rng, m, 11), _rand(rng, n, 11)
+            assert np.array_equal(oracle.comb_antidiag(a, b, 4), oracle.ref_comb(a, b, "openmp", 4)), (m, n)
+    for n in range(100, 300, 3):
+        p, q = gen.permutation(n, 60 + n, n), gen.permutation(n, 61 + n, n)
+        assert np.array_equal(oracle.steady_ant(p, q), oracle.ref_braid(p, q, "naive")), n
+    for n in range(1000, 30000, 111):
+        p, q = gen.permutation(n, 62 + n, n), gen.permutation(n, 63 + n, n)
+        assert np.array_equal(oracle.steady_ant(p, q), oracle.ref_braid(p, q, "seq")), n
+    for m in range(5, 500, 7):
+        for n in range(5, 500, 49):
+            a, b = _rand(rng, m, 15), _rand(rng, n, 15)
+            s = oracle.lcs_dp(a, b)
+            assert s == oracle.ref_lcs(a, b, "dummy") == oracle.ref_lcs(a, b, "semilocal") == oracle.ref_lcs(a, b), (m, n)
