@@ -244,6 +244,18 @@ int duplicate_search(const T *pattern, int m, const T *text, int n, double k, bo
     return SLCS_OK;
 }
 
+// int32 symbols go to the combing kernel as they are, unless they hold one of its two reserved padding codes: then
+// pattern and text are mapped to dense codes (a one-to-one map, so every match and every result stays the same).
+int duplicate_search_i32(const int32_t *pattern, int m, const int32_t *text, int n, double k, bool sparse,
+                         slcs_interval *out, int cap, int *n_out) {
+    if (m > 0 && n > 0 && pattern && text) {
+        std::vector<int32_t> cp, ct;
+        if (am::dense_codes_if_reserved(pattern, m, text, n, kSymRowVirtual, kSymColVirtual, &cp, &ct))
+            return duplicate_search<int32_t>(cp.data(), m, ct.data(), n, k, sparse, out, cap, n_out);
+    }
+    return duplicate_search<int32_t>(pattern, m, text, n, k, sparse, out, cap, n_out);
+}
+
 }  // namespace
 }  // namespace slcs
 
@@ -258,7 +270,7 @@ int slcs_duplicate_search_u8(const uint8_t *pattern, int m, const uint8_t *text,
 
 int slcs_duplicate_search_i32(const int32_t *pattern, int m, const int32_t *text, int n, double k,
                               slcs_interval *out, int out_cap, int *n_out) {
-    return duplicate_search<int32_t>(pattern, m, text, n, k, false, out, out_cap, n_out);
+    return duplicate_search_i32(pattern, m, text, n, k, false, out, out_cap, n_out);
 }
 
 int slcs_duplicate_search_sparse_u8(const uint8_t *pattern, int m, const uint8_t *text, int n, double k,
@@ -268,7 +280,7 @@ int slcs_duplicate_search_sparse_u8(const uint8_t *pattern, int m, const uint8_t
 
 int slcs_duplicate_search_sparse_i32(const int32_t *pattern, int m, const int32_t *text, int n, double k,
                                      slcs_interval *out, int out_cap, int *n_out) {
-    return duplicate_search<int32_t>(pattern, m, text, n, k, true, out, out_cap, n_out);
+    return duplicate_search_i32(pattern, m, text, n, k, true, out, out_cap, n_out);
 }
 
 }  // extern "C"

@@ -1,8 +1,9 @@
 // amatch_pick.h -- the host steps of the approximate pattern search after the device has produced, for every window
 // start over the threshold, its best interval W(i): order by window start, keep the distinct intervals in the
 // reference's order, sort them by (start, score descending) and pick greedily without overlap
-// (R:approximate_matching/ApproximateMatching.h:186-200, 261-272, 346-406).  Host-only C++, included by amatch.cu and
-// by the CPU check of these steps (tests/cpp/amatch_pick_check.cpp).
+// (R:approximate_matching/ApproximateMatching.h:186-200, 261-272, 346-406); and the map of int32 symbols away from the
+// combing kernel's reserved codes.  Host-only C++, included by amatch.cu and by the CPU check of these steps
+// (tests/cpp/amatch_pick_check.cpp).
 #pragma once
 
 #include <algorithm>
@@ -132,6 +133,30 @@ int greedy_pick(std::vector<Iv> &cand, int cap, Put put) {
         }
     }
     return cnt;
+}
+
+// Symbols are only ever compared for equality, so any one-to-one map of the values keeps every result.  When p or
+// t holds one of the two codes r0, r1 that the combing kernel reserves for padding, fills cp / ct with dense codes
+// 0..k-1 (k = number of distinct values; equal values get equal codes) and returns true; otherwise returns false and
+// leaves them untouched, and the caller passes its symbols as they are.
+inline bool dense_codes_if_reserved(const int32_t *p, int m, const int32_t *t, int n, int32_t r0, int32_t r1,
+                                    std::vector<int32_t> *cp, std::vector<int32_t> *ct) {
+    bool hit = false;
+    for (int i = 0; i < m && !hit; ++i) hit = p[i] == r0 || p[i] == r1;
+    for (int i = 0; i < n && !hit; ++i) hit = t[i] == r0 || t[i] == r1;
+    if (!hit) return false;
+    std::vector<int32_t> vals(p, p + m);
+    vals.insert(vals.end(), t, t + n);
+    std::sort(vals.begin(), vals.end());
+    vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+    auto code = [&](int32_t v) {
+        return static_cast<int32_t>(std::lower_bound(vals.begin(), vals.end(), v) - vals.begin());
+    };
+    cp->resize(m);
+    ct->resize(n);
+    for (int i = 0; i < m; ++i) (*cp)[i] = code(p[i]);
+    for (int i = 0; i < n; ++i) (*ct)[i] = code(t[i]);
+    return true;
 }
 
 }  // namespace am

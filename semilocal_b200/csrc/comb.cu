@@ -19,8 +19,6 @@
 namespace slcs {
 namespace {
 
-constexpr int kSymRowVirtual = -0x40000000;   // a-symbol of a padding row: matches nothing
-constexpr int kSymColVirtual = -0x40000001;   // b-symbol of a padding column: matches nothing
 constexpr int kStrandPad = 0x7fffffff;        // strand of a padding column: never smaller than a left strand
 
 template <typename T, int R>

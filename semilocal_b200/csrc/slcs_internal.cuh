@@ -144,6 +144,11 @@ int pick_sa_cutoff();             // steady-ant size finished in shared memory
 // ------------------------------------------------------------------------------------------------
 // combing (comb.cu)
 // ------------------------------------------------------------------------------------------------
+// Symbol codes the combing kernel reserves for its padding rows and columns (they match nothing).  int32 symbols
+// handed to it must differ from both: the host entry points map inputs that hold them to dense codes first.
+constexpr int kSymRowVirtual = -0x40000000;   // a-symbol of a padding row
+constexpr int kSymColVirtual = -0x40000001;   // b-symbol of a padding column
+
 struct CombPair {
     const void *a;        // symbols of the row string (T)
     const void *b;        // symbols of the column string (T)

@@ -2,7 +2,8 @@
 // the reference's steps: a comparison sort by window start, std::unordered_set for the distinct intervals, the
 // sort by (start, score descending) and the greedy pick (R:approximate_matching/ApproximateMatching.h:186-200,
 // 261-272, 346-406).  Random candidate sets with many repeated intervals and ties of (start, score), in the arbitrary
-// order the device's atomics leave them.  Prints "ok <cases>" or the first mismatch.
+// order the device's atomics leave them; and the map of int32 symbols away from the combing kernel's reserved codes.
+// Prints "ok <cases>" or the first mismatch.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -139,6 +140,51 @@ int main() {
                 printf("trial %d: sparse pick differs\n", trial);
                 return 1;
             }
+        }
+        ++cases;
+    }
+    // the map away from the combing kernel's reserved codes: a no-op without them, one-to-one onto 0..k-1 with them
+    const int32_t r0 = -0x40000000, r1 = -0x40000001;
+    const int32_t pool[] = {r0, r1, r0 + 1, r1 - 1, 0, 7, -7, 2147483647, -2147483647 - 1};
+    for (int trial = 0; trial < 200; ++trial) {
+        const int m = 1 + static_cast<int>(rng() % 50), n = 1 + static_cast<int>(rng() % 200);
+        std::vector<int32_t> p(m), t(n), cp, ct;   // odd trials may draw r0 / r1, even ones never do
+        for (auto &v : p) v = pool[2 + rng() % 7];
+        for (auto &v : t) v = pool[2 + rng() % 7];
+        if (trial % 2) {
+            for (int r = 0; r < 3; ++r) p[rng() % m] = pool[rng() % 9];
+            for (int r = 0; r < 5; ++r) t[rng() % n] = pool[rng() % 9];
+        }
+        bool has = false;
+        for (int32_t v : p) has |= v == r0 || v == r1;
+        for (int32_t v : t) has |= v == r0 || v == r1;
+        const bool mapped = slcs::am::dense_codes_if_reserved(p.data(), m, t.data(), n, r0, r1, &cp, &ct);
+        if (mapped != has || (!mapped && (!cp.empty() || !ct.empty()))) {
+            printf("remap trial %d: mapped %d, reserved codes present %d\n", trial, mapped, has);
+            return 1;
+        }
+        if (!mapped) continue;
+        std::vector<int32_t> all(p), codes(cp);
+        all.insert(all.end(), t.begin(), t.end());
+        codes.insert(codes.end(), ct.begin(), ct.end());
+        int32_t hi = -1;
+        for (size_t x = 0; x < all.size(); ++x) {
+            hi = std::max(hi, codes[x]);
+            if (codes[x] < 0 || codes[x] == r0 || codes[x] == r1) {
+                printf("remap trial %d: code %d out of range\n", trial, codes[x]);
+                return 1;
+            }
+            for (size_t y = 0; y < all.size(); ++y)
+                if ((all[x] == all[y]) != (codes[x] == codes[y])) {
+                    printf("remap trial %d: equality not kept\n", trial);
+                    return 1;
+                }
+        }
+        std::vector<int32_t> d(all);
+        std::sort(d.begin(), d.end());
+        if (hi + 1 != static_cast<int32_t>(std::unique(d.begin(), d.end()) - d.begin())) {
+            printf("remap trial %d: codes not dense\n", trial);
+            return 1;
         }
         ++cases;
     }

@@ -45,6 +45,18 @@ def test_random_vs_oracle(engine, oracle, symbols):
         assert engine.duplicate_search(p, t, k) == oracle.duplicate_search(p, t, k), (m, n, k)
 
 
+@pytest.mark.parametrize("sparse", [False, True])
+def test_i32_symbols_equal_to_padding_codes(engine, oracle, sparse):
+    """int32 symbols are arbitrary values compared for equality, including the two codes the combing kernel keeps
+    for its padding rows and columns (-2^30 and -2^30 - 1): the results stay the reference's."""
+    table = np.array([-(1 << 30), -(1 << 30) - 1, 5, (1 << 31) - 1], dtype=np.int64)
+    for m, n, k, seed in [(37, 3000, 0.8, 61), (200, 9000, 0.9, 62), (1, 40, 1.0, 63)]:
+        p, t = gen.planted_text(m, n, 6, 4, seed)
+        p, t = table[p].astype(np.int32), table[t].astype(np.int32)
+        assert engine.duplicate_search(p, t, k, sparse=sparse) == oracle.duplicate_search(p, t, k, sparse=sparse), \
+            (m, n, k)
+
+
 def test_edges(engine, oracle):
     # window of one end (k = 1), the text exactly one window long, a one-symbol pattern, intervals down to length 0
     for m, n, k in [(1, 50, 1.0), (40, 40, 1.0), (40, 41, 1.0), (8, 17, 0.5), (1, 9, 0.2), (3, 3000, 0.34)]:
