@@ -13,6 +13,8 @@
  *                         top strands m..m+n-1 (strand r enters at column r-m);
  *   strand ends (cols):   bottom exits 0..n-1 (column j), right exits n..n+m-1 (n+l is row m-1-l).
  * col_to_row is the inverse map.  Permutations for braid multiplication are n x n row->col maps.
+ * Sizes: a pair's m + n, a glued braid's strands and a permutation's n must be below 2^30; larger sizes return
+ * SLCS_ERR_TOO_LARGE before any device work.
  *
  * Reference interfaces replaced (paths relative to the reference project, R: = source/cpu/):
  *   semi_local::SemiLocalStrategy<Input>::compute          R:include/SemiLocal/SemiLocalLCS.h:7-11

@@ -369,6 +369,7 @@ extern "C" {
 
 int slcs_bitcomb_llcs_u8_dev(const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_score, void *stream) {
     if (m < 0 || n < 0) return fail(SLCS_ERR_ARG, "negative length");
+    if ((long long) m + n >= (1ll << 30)) return fail(SLCS_ERR_TOO_LARGE, "m + n must be below 2^30");
     if ((m > 0 && !d_a) || (n > 0 && !d_b) || !d_score) return fail(SLCS_ERR_ARG, "NULL buffer");
     Engine *E;
     SLCS_TRY(engine(&E));
@@ -378,6 +379,7 @@ int slcs_bitcomb_llcs_u8_dev(const uint8_t *d_a, int m, const uint8_t *d_b, int 
 
 int slcs_bitcomb_llcs_u8(const uint8_t *a, int m, const uint8_t *b, int n, int32_t *score) {
     if (m < 0 || n < 0) return fail(SLCS_ERR_ARG, "negative length");
+    if ((long long) m + n >= (1ll << 30)) return fail(SLCS_ERR_TOO_LARGE, "m + n must be below 2^30");
     if ((m > 0 && !a) || (n > 0 && !b) || !score) return fail(SLCS_ERR_ARG, "NULL buffer");
     for (int i = 0; i < m; ++i)
         if (a[i] > 3) return fail(SLCS_ERR_ARG, "bit-parallel combing needs symbols < 4");

@@ -490,6 +490,8 @@ using namespace slcs;
 extern "C" int slcs_staggered_glue(const int32_t *p, int pm, int pn, const int32_t *q, int qm, int qn, int row_glue,
                                    int32_t *out) {
     if (pm < 0 || pn < 0 || qm < 0 || qn < 0 || !p || !q || !out) return fail(SLCS_ERR_ARG, "bad glue arguments");
+    if ((long long) pm + pn + qm + qn >= (1ll << 30))
+        return fail(SLCS_ERR_TOO_LARGE, "the braids' strands must number below 2^30");
     const int k = row_glue ? pn : pm;
     if (row_glue ? (qn != pn) : (qm != pm)) return fail(SLCS_ERR_ARG, "the braids do not share k strands");
     const int psz = pm + pn, qsz = qm + qn;

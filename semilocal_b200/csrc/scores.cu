@@ -211,6 +211,7 @@ extern "C" {
 int slcs_scores_dev(const int32_t *d_row_to_col, int m, int n, const slcs_query *d_q, int nq, int32_t *d_out,
                     void *stream) {
     if (m < 0 || n < 0 || nq < 0) return fail(SLCS_ERR_ARG, "negative size");
+    if ((long long) m + n >= (1ll << 30)) return fail(SLCS_ERR_TOO_LARGE, "m + n must be below 2^30");
     if (nq > 0 && (!d_q || !d_out || (m + n > 0 && !d_row_to_col))) return fail(SLCS_ERR_ARG, "NULL buffer");
     Engine *E;
     SLCS_TRY(engine(&E));
@@ -226,6 +227,7 @@ int slcs_scores_dev(const int32_t *d_row_to_col, int m, int n, const slcs_query 
 
 int slcs_scores(const int32_t *row_to_col, int m, int n, const slcs_query *q, int nq, int32_t *out) {
     if (m < 0 || n < 0 || nq < 0) return fail(SLCS_ERR_ARG, "negative size");
+    if ((long long) m + n >= (1ll << 30)) return fail(SLCS_ERR_TOO_LARGE, "m + n must be below 2^30");
     if (nq == 0) return SLCS_OK;
     if (!q || !out || (m + n > 0 && !row_to_col)) return fail(SLCS_ERR_ARG, "NULL buffer");
     Engine *E;
@@ -247,6 +249,7 @@ int slcs_scores(const int32_t *row_to_col, int m, int n, const slcs_query *q, in
 int slcs_window_scores_dev(const int32_t *d_row_to_col, const int32_t *d_col_to_row, int m, int n, int w,
                            int32_t *d_out, void *stream) {
     if (m < 0 || n < 0 || w < 1 || w > n) return fail(SLCS_ERR_ARG, "window length must be in [1, n]");
+    if ((long long) m + n >= (1ll << 30)) return fail(SLCS_ERR_TOO_LARGE, "m + n must be below 2^30");
     if (!d_row_to_col || !d_out) return fail(SLCS_ERR_ARG, "NULL buffer");
     Engine *E;
     SLCS_TRY(engine(&E));
@@ -256,6 +259,7 @@ int slcs_window_scores_dev(const int32_t *d_row_to_col, const int32_t *d_col_to_
 
 int slcs_window_scores(const int32_t *row_to_col, int m, int n, int w, int32_t *out) {
     if (m < 0 || n < 0 || w < 1 || w > n) return fail(SLCS_ERR_ARG, "window length must be in [1, n]");
+    if ((long long) m + n >= (1ll << 30)) return fail(SLCS_ERR_TOO_LARGE, "m + n must be below 2^30");
     if (!row_to_col || !out) return fail(SLCS_ERR_ARG, "NULL buffer");
     Engine *E;
     SLCS_TRY(engine(&E));

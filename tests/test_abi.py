@@ -65,3 +65,25 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(_lib.Result) == 64
     assert ctypes.sizeof(_lib.ServerStats) == 96
     assert ctypes.sizeof(_lib.Tuning) == 288
+
+
+def test_sizes_beyond_the_limit_are_rejected_before_device_work():
+    """Every entry point taking a pair, a braid or a permutation refuses m + n (or n) >= 2^30 with
+    SLCS_ERR_TOO_LARGE before it touches a device, so this holds on a host without a GPU too."""
+    from semilocal_b200 import _lib
+    L = ctypes.CDLL(_lib.LIB_PATH)
+    L.slcs_last_error.restype = ctypes.c_char_p
+    big, p = 1 << 29, ctypes.c_void_p(16)   # m = n = 2^29: m + n = 2^30; p is never dereferenced
+    q = _lib.Query()
+    calls = {
+        "slcs_comb_u8": lambda: L.slcs_comb_u8(p, big, p, big, p, None, None, None),
+        "slcs_scores": lambda: L.slcs_scores(p, big, big, ctypes.byref(q), 1, p),
+        "slcs_scores_dev": lambda: L.slcs_scores_dev(p, big, big, ctypes.byref(q), 1, p, None),
+        "slcs_window_scores": lambda: L.slcs_window_scores(p, big, big, 5, p),
+        "slcs_window_scores_dev": lambda: L.slcs_window_scores_dev(p, p, big, big, 5, p, None),
+        "slcs_bitcomb_llcs_u8_dev": lambda: L.slcs_bitcomb_llcs_u8_dev(p, big, p, big, p, None),
+        "slcs_staggered_glue": lambda: L.slcs_staggered_glue(p, big, big, p, big, big, 1, p),
+        "slcs_steady_ant": lambda: L.slcs_steady_ant(p, p, 1 << 30, p, None),
+    }
+    for name, call in calls.items():
+        assert call() == 5, (name, L.slcs_last_error())
