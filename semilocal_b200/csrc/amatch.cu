@@ -248,7 +248,7 @@ int duplicate_search(const T *pattern, int m, const T *text, int n, double k, bo
 // pattern and text are mapped to dense codes (a one-to-one map, so every match and every result stays the same).
 int duplicate_search_i32(const int32_t *pattern, int m, const int32_t *text, int n, double k, bool sparse,
                          slcs_interval *out, int cap, int *n_out) {
-    if (m > 0 && n > 0 && pattern && text) {
+    if (m > 0 && n > 0 && pattern && text && (long long) m + n < (1ll << 30)) {
         std::vector<int32_t> cp, ct;
         if (am::dense_codes_if_reserved(pattern, m, text, n, kSymRowVirtual, kSymColVirtual, &cp, &ct))
             return duplicate_search<int32_t>(cp.data(), m, ct.data(), n, k, sparse, out, cap, n_out);

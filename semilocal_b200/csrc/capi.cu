@@ -312,6 +312,8 @@ int slcs_comb_u8(const uint8_t *a, int m, const uint8_t *b, int n, int32_t *row_
 int slcs_comb_i32(const int32_t *a, int m, const int32_t *b, int n, int32_t *row_to_col, int32_t *col_to_row,
                   int32_t *score, const slcs_opts *opts) {
     if (m < 0 || n < 0) return fail(SLCS_ERR_ARG, "negative length");
+    if ((m > 0 && !a) || (n > 0 && !b) || !row_to_col) return fail(SLCS_ERR_ARG, "NULL buffer");
+    if ((long long) m + n >= (1ll << 30)) return fail(SLCS_ERR_TOO_LARGE, "m + n must be below 2^30");
     // symbols are compared for equality only: map them to dense codes >= 0 (the kernel reserves
     // negative codes for padding), narrowing to uint8 when the alphabet allows it
     std::vector<int32_t> all;
@@ -358,7 +360,12 @@ int slcs_comb_u8_dev(const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32
 
 int slcs_lcs_u8(const uint8_t *a, int m, const uint8_t *b, int n, int32_t *score) {
     if (!score) return fail(SLCS_ERR_ARG, "NULL score");
-    if (m == 0 || n == 0) {
+    if (m < 0 || n < 0) return fail(SLCS_ERR_ARG, "negative length");
+    if ((m > 0 && !a) || (n > 0 && !b)) return fail(SLCS_ERR_ARG, "NULL buffer");
+    if ((long long) m + n >= (1ll << 30)) return fail(SLCS_ERR_TOO_LARGE, "m + n must be below 2^30");
+    if (m == 0 || n == 0) {   // no cells: the score is 0 (still only with a usable device, like every call)
+        Engine *E;
+        SLCS_TRY(engine(&E));
         *score = 0;
         return SLCS_OK;
     }

@@ -84,6 +84,23 @@ def test_sizes_beyond_the_limit_are_rejected_before_device_work():
         "slcs_bitcomb_llcs_u8_dev": lambda: L.slcs_bitcomb_llcs_u8_dev(p, big, p, big, p, None),
         "slcs_staggered_glue": lambda: L.slcs_staggered_glue(p, big, big, p, big, big, 1, p),
         "slcs_steady_ant": lambda: L.slcs_steady_ant(p, p, 1 << 30, p, None),
+        "slcs_comb_i32": lambda: L.slcs_comb_i32(p, big, p, big, p, None, None, None),
+        "slcs_lcs_u8": lambda: L.slcs_lcs_u8(p, big, p, big, p),
     }
     for name, call in calls.items():
         assert call() == 5, (name, L.slcs_last_error())
+
+
+def test_bad_arguments_are_status_codes_not_crashes():
+    """Negative lengths and NULL buffers come back as SLCS_ERR_ARG from the host entry points, before anything is
+    read, allocated or sent to a device."""
+    from semilocal_b200 import _lib
+    L = ctypes.CDLL(_lib.LIB_PATH)
+    L.slcs_last_error.restype = ctypes.c_char_p
+    p = ctypes.c_void_p(16)   # never dereferenced
+    score = ctypes.c_int32()
+    assert L.slcs_lcs_u8(p, -5, p, 3, ctypes.byref(score)) == 1
+    assert L.slcs_lcs_u8(None, 4, p, 3, ctypes.byref(score)) == 1
+    assert L.slcs_comb_i32(None, 4, p, 3, p, None, None, None) == 1
+    assert L.slcs_comb_i32(p, 4, None, 3, p, None, None, None) == 1
+    assert L.slcs_comb_u8(p, -1, p, 3, p, None, None, None) == 1
