@@ -78,7 +78,8 @@ int slcs_comb_u8(const uint8_t *a, int m, const uint8_t *b, int n, int32_t *row_
 /* Same for int32 symbols (Input = int in the reference); symbols are compared for equality only. */
 int slcs_comb_i32(const int32_t *a, int m, const int32_t *b, int n, int32_t *row_to_col, int32_t *col_to_row,
                   int32_t *score, const slcs_opts *opts);
-/* Device-pointer variant: all pointers are device memory, work is ordered on `stream`. */
+/* Device-pointer variant: all pointers are device memory, work is ordered on `stream`.  d_row_to_col is
+ * required; d_col_to_row and d_score are optional. */
 int slcs_comb_u8_dev(const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_row_to_col,
                      int32_t *d_col_to_row, int32_t *d_score, const slcs_opts *opts, void *stream);
 /* Allocation-free variant of slcs_comb_u8_dev, for callers that cannot let the engine allocate device

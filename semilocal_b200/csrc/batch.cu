@@ -201,6 +201,7 @@ int slcs_batch_upload(slcs_batch *bt, const uint8_t *a_cat, const int64_t *a_off
         a_len = std::max<int64_t>(a_len, a_off[i] + bt->m[i]);
         b_len = std::max<int64_t>(b_len, b_off[i] + bt->n[i]);
     }
+    if ((a_len > 0 && !a_cat) || (b_len > 0 && !b_cat)) return fail(SLCS_ERR_ARG, "NULL strings");
     if (a_len > bt->a_len || !bt->da) {
         if (bt->da) dfree(bt->da, s);
         bt->da = nullptr;

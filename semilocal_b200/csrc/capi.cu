@@ -339,6 +339,8 @@ int slcs_comb_i32(const int32_t *a, int m, const int32_t *b, int n, int32_t *row
 int slcs_comb_u8_dev(const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_row_to_col,
                      int32_t *d_col_to_row, int32_t *d_score, const slcs_opts *opts, void *stream) {
     if (m < 0 || n < 0) return fail(SLCS_ERR_ARG, "negative length");
+    if ((m > 0 && !d_a) || (n > 0 && !d_b) || (m + n > 0 && !d_row_to_col))
+        return fail(SLCS_ERR_ARG, "NULL buffer (d_row_to_col is required)");
     if ((long long) m + n >= (1ll << 30)) return fail(SLCS_ERR_TOO_LARGE, "m + n must be below 2^30");
     Engine *E;
     SLCS_TRY(engine(&E));

@@ -104,3 +104,5 @@ def test_bad_arguments_are_status_codes_not_crashes():
     assert L.slcs_comb_i32(None, 4, p, 3, p, None, None, None) == 1
     assert L.slcs_comb_i32(p, 4, None, 3, p, None, None, None) == 1
     assert L.slcs_comb_u8(p, -1, p, 3, p, None, None, None) == 1
+    assert L.slcs_comb_u8_dev(p, 4, p, 3, None, None, None, None, None) == 1   # the device output is required
+    assert L.slcs_comb_u8_dev(None, 4, p, 3, p, None, None, None, None) == 1
