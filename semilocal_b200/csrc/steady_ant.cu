@@ -1661,6 +1661,7 @@ struct slcs_sa_plan {
     SaPlan *plan = nullptr;
     int *d_err = nullptr;
     int device = 0;
+    int n = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     const void *gp = nullptr, *gq = nullptr, *gr = nullptr;
@@ -1673,6 +1674,7 @@ int slcs_sa_plan_create(int n, slcs_sa_plan **out) {
     SLCS_TRY(engine(&E));
     auto h = new slcs_sa_plan();
     h->device = E->device;
+    h->n = n;
     int rc = sa_plan_create(std::vector<int64_t>{0}, std::vector<int>{n}, &h->plan, E->stream, nullptr);
     if (rc == SLCS_OK) rc = dalloc(reinterpret_cast<void **>(&h->d_err), sizeof(int), E->stream);
     if (rc == SLCS_OK && cudaMemsetAsync(h->d_err, 0, sizeof(int), E->stream) != cudaSuccess) rc = SLCS_ERR_CUDA;
@@ -1688,6 +1690,7 @@ int slcs_sa_plan_create(int n, slcs_sa_plan **out) {
 int slcs_sa_plan_run(slcs_sa_plan *h, const int32_t *d_p, const int32_t *d_q, int32_t *d_r, int use_graph,
                      void *stream) {
     if (!h) return fail(SLCS_ERR_ARG, "NULL plan");
+    if (h->n > 0 && (!d_p || !d_q || !d_r)) return fail(SLCS_ERR_ARG, "NULL buffer");
     SLCS_CUDA_TRY(cudaSetDevice(h->device));
     Engine *E;
     SLCS_TRY(engine(&E));
