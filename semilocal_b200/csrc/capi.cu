@@ -6,6 +6,7 @@
 #include <numeric>
 
 #include "slcs_internal.cuh"
+#include "symbol_codes.h"
 
 namespace slcs {
 
@@ -314,8 +315,14 @@ int slcs_comb_i32(const int32_t *a, int m, const int32_t *b, int n, int32_t *row
     if (m < 0 || n < 0) return fail(SLCS_ERR_ARG, "negative length");
     if ((m > 0 && !a) || (n > 0 && !b) || !row_to_col) return fail(SLCS_ERR_ARG, "NULL buffer");
     if ((long long) m + n >= (1ll << 30)) return fail(SLCS_ERR_TOO_LARGE, "m + n must be below 2^30");
-    // symbols are compared for equality only: map them to dense codes >= 0 (the kernel reserves
-    // negative codes for padding), narrowing to uint8 when the alphabet allows it
+    // symbols are compared for equality only: map them to codes >= 0 (the kernel reserves negative codes for
+    // padding) -- v - min as uint8 when the symbols span at most 256 values, else dense codes, narrowed to uint8
+    // when at most 256 values occur
+    {
+        std::vector<uint8_t> ca, cb;
+        if (range_codes_u8(a, m, b, n, &ca, &cb))
+            return comb_host<uint8_t>(ca.data(), m, cb.data(), n, row_to_col, col_to_row, score, opts);
+    }
     std::vector<int32_t> all;
     all.reserve((size_t) m + n);
     if (m) all.insert(all.end(), a, a + m);

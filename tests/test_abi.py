@@ -106,3 +106,15 @@ def test_bad_arguments_are_status_codes_not_crashes():
     assert L.slcs_comb_u8(p, -1, p, 3, p, None, None, None) == 1
     assert L.slcs_comb_u8_dev(p, 4, p, 3, None, None, None, None, None) == 1   # the device output is required
     assert L.slcs_comb_u8_dev(None, 4, p, 3, p, None, None, None, None) == 1
+
+
+def test_int32_symbol_map(tmp_path):
+    """The int32 combing entry point's symbol map (semilocal_b200/csrc/symbol_codes.h) applies exactly when the
+    symbols span at most 256 values and keeps every (in)equality between them (tests/cpp/symbol_codes_check.cpp)."""
+    import subprocess
+    exe = str(tmp_path / "symbol_codes_check")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror", "-I",
+                    os.path.join(ROOT, "semilocal_b200", "csrc"), os.path.join(ROOT, "tests", "cpp", "symbol_codes_check.cpp"),
+                    "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout + r.stderr
