@@ -118,7 +118,8 @@ def test_reference_test_grids(oracle):
     and alphabets as there; strings and permutations seeded here): SemiLocalLCSTest.cpp:47-55 (Dummy vs Simple,
     5..49 squared, 5 letters) and :57-68 (Simple vs OpenMP, 4900..4999 step 11, 11 letters), SteadyAntTest.cpp:
     43-56 (Naive vs SimpleSticky, 100..299, every 3rd size here) and :59-67 (SimpleSticky vs MemoryOptimized, 1000..29999 step 111),
-    LCSTest.cpp:65-86 (Dummy vs SemiLocal vs SequentialMem, 5..499 with 15 letters; every 7th size pair here)."""
+    LCSTest.cpp:65-86 (Dummy vs SemiLocal vs SequentialMem, 5..499 with 15 letters; every 7th size pair here), and the
+    combined and hybrid strategies of SemiLocalLCSTest.cpp:88-130 on parts of their grids."""
     rng = np.random.default_rng(50)
     for m in range(5, 50):
         for n in range(5, 50):
@@ -141,3 +142,14 @@ def test_reference_test_grids(oracle):
             a, b = _rand(rng, m, 15), _rand(rng, n, 15)
             s = oracle.lcs_dp(a, b)
             assert s == oracle.ref_lcs(a, b, "dummy") == oracle.ref_lcs(a, b, "semilocal") == oracle.ref_lcs(a, b), (m, n)
+    # SemiLocalLCSTest.cpp:88-130: OpenMP vs Combined (3000..3339, 150 letters), vs HybridRecursive (3900..3999) and
+    # vs HybridIterative (one 10^5 pair there; 20000 here, tiles 4096), every few sizes of each grid
+    for m in range(3000, 3340, 110):
+        for n in range(3000, 3340, 110):
+            a, b = _rand(rng, m, 150), _rand(rng, n, 150)
+            assert np.array_equal(oracle.comb_antidiag(a, b, 4), oracle.ref_comb(a, b, "combined", 2)), (m, n)
+    for m, n in [(3900, 3955), (3977, 3911)]:
+        a, b = _rand(rng, m, 150), _rand(rng, n, 150)
+        assert np.array_equal(oracle.comb_antidiag(a, b, 4), oracle.ref_hybrid_recursive(a, b, 2, 6, 400)), (m, n)
+    a, b = _rand(rng, 20000, 150), _rand(rng, 20037, 150)
+    assert np.array_equal(oracle.comb_antidiag(a, b, 8), oracle.ref_hybrid_iterative(a, b, 4, 4096, 4096))
