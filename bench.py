@@ -27,7 +27,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from semilocal_b200 import gen  # noqa: E402
-from semilocal_b200.shard import max_over_ranks  # noqa: E402
+from semilocal_b200.shard import max_over_ranks, shard_pairs  # noqa: E402
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 OPS_PER_CELL = 5     # compare, compare, or, two selects (R:include/SemiLocal/SemiLocalLCS.h:158-172)
@@ -35,6 +35,12 @@ OPS_PER_CELL = 5     # compare, compare, or, two selects (R:include/SemiLocal/Se
 # (`python -m semilocal_b200.profile_cases batch 256`: 3.29 MB for 8.12e9 cells); a launch's traffic grows with
 # its bands x columns, i.e. with its cells at a fixed band height, so the bench scales it by cells.
 COMB_DRAM_BYTES_PER_CELL = 3.29e6 / 8.1177e9
+# Pipe split of comb_kernel from ncu (profiles/comb_kernel_batch_2048_pairs.md): the ALU pipe carries the cell's
+# compares and selects, the FMA pipe is idle; the issue slots are half used.
+COMB_PIPE_SPLIT = {"alu_pct_of_peak": 80.2, "fma_pct_of_peak": 0.77, "issue_pct": 46.6,
+                   "source": "ncu --set full, comb_kernel, 2048-pair batch (profiles/comb_kernel_batch_2048_pairs.md)"}
+SM_COUNT = 148
+DIGESTS_PATH = os.path.join(ROOT, "tests", "golden", "headline_digests.json")
 
 
 def dist_env():
@@ -98,6 +104,56 @@ class Clocks:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def issue_ceiling_gops(clocks) -> float:
+    """Integer-op ceiling of the SM issue slots: every SMSP issues one warp instruction (32 lane-ops) per clock,
+    at the median SM clock sampled under load (the maximum clock when no sample was taken)."""
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    return SM_COUNT * 4 * 32 * mhz * 1e6 / 1e9
+
+
+def check_against_reference(braids, scores, ms, ns, shard):
+    """Every braid of a timed batch against the digests of the reference's results on the seed-5 batch
+    (OpenMPIterativeCombing<int,false>(1) per pair, tests/golden/headline_digests.json).  `shard` maps the
+    plan's pairs to indices of that batch (None: not that batch)."""
+    import hashlib
+    if shard is None:
+        return {"bit_exact_vs_reference": None, "checked_pairs": 0,
+                "note": "this rank's batch has another seed; checked against the per-pair launches only"}
+    try:
+        with open(DIGESTS_PATH) as f:
+            ref = json.load(f)["batch_4096"]
+    except (OSError, KeyError, ValueError) as e:
+        return {"bit_exact_vs_reference": None, "checked_pairs": 0, "note": f"no reference digests: {e}"}
+    off = 0
+    bad = []
+    for k, i in enumerate(shard):
+        sz = int(ms[k]) + int(ns[k])
+        d = hashlib.sha256(np.ascontiguousarray(braids[off:off + sz], dtype="<i4").tobytes()).hexdigest()
+        if d[:16] != ref["pair_sha256_16"][i] or int(scores[k]) != ref["global_scores"][i]:
+            bad.append(i)
+        off += sz
+    return {"bit_exact_vs_reference": not bad, "checked_pairs": len(shard), "mismatched_pairs": bad[:16],
+            "reference": "sha256 of each pair's int32 braid from OpenMPIterativeCombing<int,false>(1), "
+                         "the reference compiled from its sources (tests/golden/headline_digests.json)"}
+
+
+def check_pair_2p20(braids, bit_score, m, n):
+    """The 2^20 pair's braids against the digest of the reference's OpenMPHybridIterative braid and its bit
+    score against the reference braid's global score (tests/golden/headline_digests.json)."""
+    import hashlib
+    try:
+        with open(DIGESTS_PATH) as f:
+            ref = json.load(f)["hybrid_2p20"]
+    except (OSError, KeyError, ValueError) as e:
+        return {"note": f"no reference digests: {e}"}
+    out = {name + "_bit_exact_vs_reference":
+           hashlib.sha256(np.ascontiguousarray(r, dtype="<i4").tobytes()).hexdigest() == ref["sha256"]
+           for name, r in braids.items()}
+    out["bit_parallel_score_equals_reference"] = int(bit_score) == ref["global_score"] and (m, n) == (ref["m"], ref["n"])
+    out["reference"] = "OpenMPHybridIterative<int,false>(threads, 4096, 4096), the reference compiled from its sources"
+    return out
 
 
 def load_peaks():
@@ -188,7 +244,18 @@ def run_ours(args, rank, world, local):
     t_tune = time.perf_counter()
     table = S.autotune(cache=args.tuning_cache or None)
     t_tune = time.perf_counter() - t_tune
-    pairs = batch_workload(5 + 1000 * rank)
+    if args.shard == "fixed":
+        # one batch for the whole job, split over the ranks by cost; no data-path collective
+        full = batch_workload(5)
+        shard = shard_pairs([len(a) * len(b) for a, b in full], world)[rank]
+        pairs = [full[i] for i in shard]
+        job_cells = sum(len(a) * len(b) for a, b in full)
+        del full
+    else:
+        # weak scaling: every rank its own batch (rank 0 the seed the reference digests are taken on)
+        pairs = batch_workload(5 + 1000 * rank)
+        shard = list(range(len(pairs))) if rank == 0 else None
+        job_cells = None
     a_cat, a_off, ms, b_cat, b_off, ns = S.concat_pairs(pairs)
     # pinned host copies for the end-to-end leg
     a_pin = torch.from_numpy(a_cat).pin_memory()
@@ -224,14 +291,21 @@ def run_ours(args, rank, world, local):
         ev1.synchronize()
         barrier()
     total_ms = ev0.elapsed_time(ev1)
-    # per-launch kernel time of the combing kernel (last step's events, on the launching stream)
-    kern_ms.append(plan.kernel_ms())
-    # correctness spot check of the timed plan against the oracle on a few pairs
-    plan.download(out_pin.numpy(), sc_pin.numpy(), sh)
-    torch.cuda.synchronize()
     t_max = max_over_ranks(total_ms, dist, "cuda")
     ms_per_step = t_max / args.steps
-    value = cells * world / (ms_per_step * 1e-3) / 1e9
+    value = (job_cells if job_cells is not None else cells * world) / (ms_per_step * 1e-3) / 1e9
+    # the braids of the timed plan: every one against the reference's digests (pairs of the seed-5 batch)
+    plan.download(out_pin.numpy(), sc_pin.numpy(), sh)
+    torch.cuda.synchronize()
+    braids = out_pin.numpy().copy()
+    scores = sc_pin.numpy().copy()
+    parity = check_against_reference(braids, scores, ms, ns, shard)
+    # per-launch time of the combing kernel: the mean over replays, each read from the events recorded
+    # around the kernel on the launching stream inside the graph
+    for _ in range(args.steps):
+        plan.run(use_graph=True, stream=sh)
+        stream.synchronize()
+        kern_ms.append(plan.kernel_ms())
 
     # ---- end to end through the public API: pinned H2D, run, D2H of braids + scores, every step ----
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -250,7 +324,7 @@ def run_ours(args, rank, world, local):
         e1.record(stream)
     e1.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, dist, "cuda")
-    e2e_value = cells * world / (e2e_ms * 1e-3) / 1e9
+    e2e_value = (job_cells if job_cells is not None else cells * world) / (e2e_ms * 1e-3) / 1e9
 
     # ---- plain per-pair launches on the same plan (baseline for the batched launch) ----
     plain = S.BatchPlan(ms, ns, mode=1)
@@ -267,23 +341,31 @@ def run_ours(args, rank, world, local):
     plain_ms = p0.elapsed_time(p1)
     plain_gcups = cells / (plain_ms * 1e-3) / 1e9
     plain_info = plain.info()
+    plain.download(out_pin.numpy(), sc_pin.numpy(), sh)
+    torch.cuda.synchronize()
+    parity["per_pair_launches_equal_batched"] = bool(np.array_equal(out_pin.numpy(), braids) and
+                                                     np.array_equal(sc_pin.numpy(), scores))
     plain.close()
 
     # ---- roofline of the combing kernel ----
     peak_cells = ctypes.c_double(0)
     S._lib.check(S.lib().slcs_probe_cell_peak(ctypes.byref(peak_cells)))
-    k_ms = float(np.median(kern_ms))
+    k_ms = float(np.mean(kern_ms))
     achieved_gops = OPS_PER_CELL * cells / (k_ms * 1e-3) / 1e9
     peak_gops = OPS_PER_CELL * peak_cells.value / 1e9
+    clk_summary = clk.summary()
+    issue_peak_gops = issue_ceiling_gops(clk_summary)
 
     result = {
         "metric": "GCUPS", "value": round(value, 2), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded splitmix64)",
+        "scaling": "strong" if args.shard == "fixed" else "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded splitmix64)",
         "config": {"workload": "batched combing: 4096 pairs per GPU, |a| log-uniform [256, 65536], 4 letters, "
                                "b = a with 10% subst + 1% indels; int32 braids; persistent length-bucketed "
                                "launch replayed from a CUDA graph",
-                   "pairs_per_gpu": len(pairs), "cells_per_gpu": cells, "parallelism": f"pairs sharded, {world} GPU",
+                   "pairs_per_gpu": len(pairs), "cells_per_gpu": cells,
+                   "parallelism": (f"one 4096-pair batch split by cost over {world} GPU" if args.shard == "fixed"
+                                   else f"a 4096-pair batch per GPU, {world} GPU"),
                    "l2": "inputs + braids (~%d MB) exceed the 126 MB L2" % ((a_cat.nbytes + b_cat.nbytes + 8 * plan.total) >> 20),
                    "tuning": {"band_rows_by_log2_len": {str(k): table["band_rows_batch"][k] for k in range(8, 17)},
                               "hybrid_tile": table["tile"], "steady_ant_cutoff": table["sa_cutoff"],
@@ -291,6 +373,7 @@ def run_ours(args, rank, world, local):
         "e2e": {"value": round(e2e_value, 2), "unit": "GCUPS", "h2d_bytes_per_step": info["h2d_bytes"],
                 "d2h_bytes_per_step": info["d2h_bytes"]},
         "gpu_launches": info["launches"] * args.steps,
+        "parity": parity,
         "plain_per_pair": {"value": round(plain_gcups, 2), "unit": "GCUPS", "launches": plain_info["launches"],
                            "batched_over_plain": round(value / world / plain_gcups, 2)},
         "roofline": {"bound": "int32-issue", "achieved": round(achieved_gops, 1), "peak": round(peak_gops, 1),
@@ -299,8 +382,14 @@ def run_ours(args, rank, world, local):
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of comb_kernel on the "
                                        "256-pair batch case, scaled to this launch by cells",
                      "kernel": "comb_kernel", "kernel_ms": round(k_ms, 3),
-                     "peak_source": "slcs_probe_cell_peak (cell instruction mix, full occupancy), x5 ops/cell"},
-        "clocks": clk.summary(),
+                     "kernel_ms_source": f"mean of {len(kern_ms)} graph replays' kernel events",
+                     "peak_source": "slcs_probe_cell_peak (cell instruction mix, full occupancy), x5 ops/cell",
+                     "issue_ceiling": {"peak": round(issue_peak_gops, 1), "unit": "Gop/s",
+                                       "frac": round(achieved_gops / issue_peak_gops, 4),
+                                       "source": "148 SM x 4 SMSP x 32 lanes x median SM clock, one lane-op "
+                                                 "per issue slot, x5 ops/cell"},
+                     "pipes": COMB_PIPE_SPLIT},
+        "clocks": clk_summary,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         c_cells, c_s, kind, desc = cpu_reference_batch_sample(pairs, args.cpu_budget, os.cpu_count() or 1)
@@ -439,6 +528,7 @@ def run_suite(torch, S, peak_cells, peaks):
         pl.close()
     res["hybrid_equals_wavefront"] = bool(np.array_equal(braids["hybrid_tiles_4096"], braids["wavefront"]))
     res["scores_agree"] = len({res[k]["score"] for k in ("hybrid_tiles_4096", "wavefront", "bit_parallel")}) == 1
+    res["parity"] = check_pair_2p20(braids, res["bit_parallel"]["score"], m, n)
     # the reference's hybrid on a bounded sample: the leading 2^16 x 2^16 corner of the same pair
     sa, sb = a[:1 << 16].astype(np.int32), b[:1 << 16].astype(np.int32)
     if use_ref:
@@ -619,6 +709,9 @@ def main():
     ap.add_argument("--no-suite", action="store_true", help="skip the plain / steady-ant / hybrid workloads")
     ap.add_argument("--tuning-cache", default="", help="JSON file: load the autotuned table if saved there for "
                                                         "this device, else measure and save it")
+    ap.add_argument("--shard", default="weak", choices=["weak", "fixed"],
+                    help="weak: every rank combs its own 4096-pair batch; fixed: one 4096-pair batch split over "
+                         "the ranks by cost (strong scaling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -16,8 +16,9 @@
 // They are templates over the permutation type: slcs::Permutation below (the shape of common::Permutation,
 // R:common/include/Permutations/Matrices.h:16-96) or the reference's own common::Permutation -- anything with
 // a (rows, cols) constructor, public rows/cols/m/n, set(row, col) and getColByRow(row).  A reference subclass of
-// SemiLocalStrategy / MemoryOptimizedStickBraidMultiplication forwards its virtual to these (INTEGRATION.md
-// shows the few lines).  Failures throw slcs::Error (status code + message); the engine never exits or aborts.
+// SemiLocalStrategy / MemoryOptimizedStickBraidMultiplication forwards its virtual to these in a few lines
+// (tests/cpp/reference_plugin.cpp does so).  Failures throw slcs::Error (status code + message); the engine never
+// exits or aborts.
 #pragma once
 
 #include <cstdint>
