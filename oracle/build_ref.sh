@@ -27,6 +27,11 @@ echo "build_ref: wrote $here/_ref/libslcs_ref.so"
   -I"$src" "$here/ref_am_shim.cpp" -o "$here/_ref/libslcs_ref_am.so.tmp" -Wl,--no-undefined
 mv "$here/_ref/libslcs_ref_am.so.tmp" "$here/_ref/libslcs_ref_am.so"
 echo "build_ref: wrote $here/_ref/libslcs_ref_am.so"
+# The legacy combing, steady ant and hybrid (source/cpu/semi_local.h, unit_monge_mult/steady_ant.h): second oracle
+/usr/bin/g++ -std=c++17 -O3 -march=x86-64-v3 -fopenmp -fPIC -shared -w \
+  -I"$src" "$here/ref_legacy_shim.cpp" -o "$here/_ref/libslcs_ref_legacy.so.tmp" -Wl,--no-undefined
+mv "$here/_ref/libslcs_ref_legacy.so.tmp" "$here/_ref/libslcs_ref_legacy.so"
+echo "build_ref: wrote $here/_ref/libslcs_ref_legacy.so"
 # Two of the reference's own benchmark executables (its harness protocol: R:utils/runners.py), as the pin of the
 # harness runners in semilocal_b200/harness/.
 for f in semi_local_naive_iterative semi_local_hybrid_iterative; do

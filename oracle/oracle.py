@@ -1,10 +1,11 @@
 """ctypes face of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
 
-Two libraries are wrapped:
+The libraries wrapped:
   * liboracle.so   -- the C restatement in oracle/slcs_oracle.c (always built; `make -C oracle`);
   * _ref/libslcs_ref.so -- the reference's own headers compiled by oracle/build_ref.sh (present when the
     reference sources were available at build time; the file travels with the repository snapshot);
-  * _ref/libslcs_ref_am.so -- the reference's approximate pattern search, compiled the same way.
+  * _ref/libslcs_ref_am.so -- the reference's approximate pattern search, compiled the same way;
+  * _ref/libslcs_ref_legacy.so -- the reference's legacy combing, steady ant and hybrid (second oracle).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may import this module.
 """
@@ -21,6 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libslcs_ref.so")
 REF_AM_PATH = os.path.join(HERE, "_ref", "libslcs_ref_am.so")
+REF_LEGACY_PATH = os.path.join(HERE, "_ref", "libslcs_ref_legacy.so")
 
 _lock = threading.Lock()
 _lib = None
@@ -31,6 +33,7 @@ _i32p = ctypes.POINTER(ctypes.c_int32)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _f64p = ctypes.POINTER(ctypes.c_double)
 _ref_am = None
+_ref_legacy = None
 
 
 def build() -> str:
@@ -368,3 +371,46 @@ def ref_duplicate_search(pattern, text, k: float, kind: str = "dense"):
     """The reference's own InteractiveDuplicateSearchSemiDense (kind "dense") or ...SemiSparse ("sparse")."""
     R = ref_am()
     return _intervals(R.ref_dup_search_dense if kind == "dense" else R.ref_dup_search_sparse, pattern, text, k)
+
+
+# --------------------------------------------------------------------------------------------------
+# The reference's legacy implementations (second oracle; oracle/ref_legacy_shim.cpp)
+# --------------------------------------------------------------------------------------------------
+
+def ref_legacy():
+    """The reference's legacy combing / steady ant / hybrid (R:semi_local.h, R:unit_monge_mult/steady_ant.h)
+    compiled from its sources, or None when it was not built."""
+    global _ref_legacy
+    with _lock:
+        if _ref_legacy is None and os.path.exists(REF_LEGACY_PATH):
+            R = ctypes.CDLL(REF_LEGACY_PATH)
+            R.ref_legacy_sticky_braid_mpi.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int, _i32p]
+            R.ref_legacy_steady_ant.argtypes = [_i32p, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i32p]
+            R.ref_legacy_hybrid_iterative.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int,
+                                                      ctypes.c_int, _i32p]
+            _ref_legacy = R
+    return _ref_legacy
+
+
+def legacy_comb(a, b, threads: int = 1) -> np.ndarray:
+    """semi_local::sticky_braid_mpi<int, false, false> (R:semi_local.h:212-276)."""
+    a, b = _i32(a), _i32(b)
+    out = np.empty(len(a) + len(b), dtype=np.int32)
+    ref_legacy().ref_legacy_sticky_braid_mpi(_p(a), len(a), _p(b), len(b), threads, _p(out))
+    return out
+
+
+def legacy_steady_ant(p, q, nested_lvls: int = 3, precalc: int = 5) -> np.ndarray:
+    """steady_ant_parallel_wrapper (R:unit_monge_mult/steady_ant.h:811-844)."""
+    p, q = _i32(p), _i32(q)
+    out = np.empty(len(p), dtype=np.int32)
+    ref_legacy().ref_legacy_steady_ant(_p(p), _p(q), len(p), nested_lvls, precalc, _p(out))
+    return out
+
+
+def legacy_hybrid_iterative(a, b, threads: int = 4, precalc: int = 5) -> np.ndarray:
+    """semi_local::hybrid_iterative_wrapper<false> (R:semi_local.h:740-790): symbols as unsigned short."""
+    a, b = _i32(a), _i32(b)
+    out = np.empty(len(a) + len(b), dtype=np.int32)
+    ref_legacy().ref_legacy_hybrid_iterative(_p(a), len(a), _p(b), len(b), threads, precalc, _p(out))
+    return out

@@ -153,3 +153,38 @@ def test_reference_test_grids(oracle):
         assert np.array_equal(oracle.comb_antidiag(a, b, 4), oracle.ref_hybrid_recursive(a, b, 2, 6, 400)), (m, n)
     a, b = _rand(rng, 20000, 150), _rand(rng, 20037, 150)
     assert np.array_equal(oracle.comb_antidiag(a, b, 8), oracle.ref_hybrid_iterative(a, b, 4, 4096, 4096))
+
+
+legacy_only = pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref",
+                                                                  "libslcs_ref_legacy.so")),
+                                 reason="legacy reference library oracle/_ref not built (needs the reference sources)")
+
+
+@legacy_only
+def test_legacy_second_oracle(oracle):
+    """The reference's legacy implementations (R:semi_local.h, R:unit_monge_mult/steady_ant.h) as a second oracle,
+    on the same grids as test_reference_test_grids: sticky_braid_mpi (:212-276) against the restatement on the
+    5..49 squared grid (1 and 3 threads) and the 4900..4999 grid; steady_ant_parallel_wrapper (:811-844), nested
+    and sequential, against the restatement on 100..299 and 1000..29999; hybrid_iterative_wrapper (:740-790) on a
+    pair above its 32000-row tile bound."""
+    rng = np.random.default_rng(51)
+    for m in range(5, 50, 2):
+        for n in range(5, 50, 3):
+            a, b = _rand(rng, m, 5), _rand(rng, n, 5)
+            x = oracle.comb_rowmajor(a, b)
+            assert np.array_equal(x, oracle.legacy_comb(a, b, 1)), (m, n)
+            assert np.array_equal(x, oracle.legacy_comb(a, b, 3)), (m, n)
+    for m in range(4900, 5000, 33):
+        for n in range(4900, 5000, 33):
+            a, b = _rand(rng, m, 11), _rand(rng, n, 11)
+            assert np.array_equal(oracle.comb_antidiag(a, b, 4), oracle.legacy_comb(a, b, 4)), (m, n)
+    for n in range(100, 300, 7):
+        p, q = gen.permutation(n, 70 + n, n), gen.permutation(n, 71 + n, n)
+        assert np.array_equal(oracle.steady_ant(p, q), oracle.legacy_steady_ant(p, q, 3, 5)), n
+    for n in range(1000, 30000, 1111):
+        p, q = gen.permutation(n, 72 + n, n), gen.permutation(n, 73 + n, n)
+        exp = oracle.steady_ant(p, q)
+        assert np.array_equal(exp, oracle.legacy_steady_ant(p, q, 3, 5)), n
+        assert np.array_equal(exp, oracle.legacy_steady_ant(p, q, 0, 5)), n
+    a, b = _rand(rng, 40000, 4), _rand(rng, 33001, 4)
+    assert np.array_equal(oracle.comb_antidiag(a, b, 8), oracle.legacy_hybrid_iterative(a, b, 4))
