@@ -88,9 +88,12 @@ int slcs_comb_u8_dev(const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32
  * No counterpart in the reference.
  * Its scratch is one static device array of about 192 KiB per device (held until the process exits),
  * shared by every call and cleared by each call: calls that overlap on the GPU race, so serialise them.
- * The first call on a device resolves the array's address; make it before any stream capture.
+ * The first call on a device resolves the array's address; make it before any stream capture, and do not
+ * call this entry point again after cudaDeviceReset (the address belongs to the reset context).
  * The caller passes inputs and both outputs (d_col_to_row is required; it is also the band hand-off);
- * d_score is optional.  Limits: m <= 8388608 rows (8192 bands), m + n < 2^30, else SLCS_ERR_TOO_LARGE. */
+ * d_score is optional.  Limits: m <= 8388608 rows (8192 bands), m + n < 2^30, else SLCS_ERR_TOO_LARGE.
+ * Above about 1.8 million rows the bands outnumber the resident warps and the call takes about twice as
+ * long as slcs_comb_u8_dev; pass the shorter string as a. */
 int slcs_comb_u8_dev_noalloc(const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_row_to_col,
                              int32_t *d_col_to_row, int32_t *d_score, void *stream);
 

@@ -16,9 +16,14 @@
 //    host threads on one device) race on it: serialise them.
 //  * The first call on a device resolves the array's device address (cudaGetSymbolAddress) with that
 //    device current and caches it; make that first call before any stream capture.
+//  * The cached address belongs to the device's current context: after cudaDeviceReset (or any teardown of the
+//    primary context) the process must not call this entry point again.
 //  * Limits: at most kNoAllocMaxBands bands of 32*R rows (R = 32 for long strings), i.e. m <= 8,388,608
 //    rows; m + n < 2^30.  Larger inputs are rejected with SLCS_ERR_TOO_LARGE.  The strings keep the
 //    orientation given (rows = a).
+//  * Speed: above about 1.8 million rows (m / 1024 bands beyond the ~1776 warps resident on a B200) the later
+//    bands start only when a warp has finished a whole band, which roughly doubles the time; pass the shorter
+//    string as a, or use slcs_comb_u8_dev, for such pairs.
 #include <mutex>
 
 #include "slcs_internal.cuh"
@@ -128,7 +133,13 @@ extern "C" int slcs_comb_u8_dev_noalloc(const uint8_t *d_a, int m, const uint8_t
     DeviceSetup *S;
     SLCS_TRY(setup_device(&S));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (m + n == 0) return SLCS_OK;
+    if (m + n == 0) {   // no strands: only the score (0), as the regular entry point writes it
+        if (d_score) {
+            SLCS_CUDA_TRY(cudaMemsetAsync(d_score, 0, sizeof(int32_t), s));
+            SLCS_CUDA_TRY(cudaStreamSynchronize(s));
+        }
+        return SLCS_OK;
+    }
     if (m == 0 || n == 0) {   // the identity braid needs no scratch
         noalloc_identity_kernel<<<(m + n + 255) / 256, 256, 0, s>>>(d_row_to_col, d_col_to_row, d_score, m + n);
         SLCS_CUDA_TRY(cudaGetLastError());

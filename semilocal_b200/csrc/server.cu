@@ -151,6 +151,7 @@ struct Req {
     int64_t keep = 0;   // device bytes of the resident braid
     int R = 32;         // rows per lane of the request's bands
     int nbands = 0;
+    int retries = 0;    // launches of this request that ended in a device-side wait timeout
     double t_submit = 0, t_admit = 0;
     uint8_t *ha = nullptr;   // pinned staging: a then b
     size_t hcap = 0;
@@ -389,9 +390,22 @@ bool retire(slcs_server *S) {
             st = SLCS_ERR_INTERNAL;
         }
         const double t = S->now();
+        std::vector<Req *> again;
         for (size_t i = 0; i < L->reqs.size(); ++i) {
             Req *r = L->reqs[i];
             dfree(r->dab, L->s);
+            if (st == SLCS_ERR_TIMEOUT && r->retries == 0) {
+                // a bounded wait gave up (the context was held off the GPU for seconds, e.g. time-sliced with
+                // another process): the launch's work is incomplete, so the request goes back to the front of
+                // the queue once, with its staged inputs, and is admitted again like a new one
+                dfree(r->dr2c, L->s);
+                r->dab = nullptr;
+                r->dr2c = nullptr;
+                ++r->retries;
+                unreserve(S, r->need);
+                again.push_back(r);
+                continue;
+            }
             {
                 std::lock_guard<std::mutex> lk(S->rmu);
                 S->used -= r->need - r->keep;
@@ -410,6 +424,7 @@ bool retire(slcs_server *S) {
             std::lock_guard<std::mutex> lk(S->mu);
             S->inflight_count -= (int) L->reqs.size();
         }
+        for (auto it = again.rbegin(); it != again.rend(); ++it) S->pending.push_front(*it);
         dfree(L->dmeta, L->s);
         S->pinned.put(L->hmeta, L->hcap);
         cudaEventDestroy(L->done);

@@ -72,3 +72,46 @@ def test_two_gloo_ranks_shard_time_and_gather():
     idx = sorted(i for part in gathered for i, _ in part)
     assert idx == list(range(len(costs)))                 # every pair's result reached rank 0 exactly once
     assert out[0][2] + out[1][2] == len(costs)
+
+
+def _fixed_shard_rank(rank, world, port, q):
+    """One rank of bench.py --shard fixed on the host: the whole seed-5 batch, this rank's cost shard of it."""
+    import datetime
+
+    import torch.distributed as dist
+
+    from semilocal_b200 import gen
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        costs = [len(a) * len(b) for a, b in gen.batch_pairs(4096, 256, 65536, seed=5)]   # as bench.py does
+        mine = shard_pairs(costs, world)[rank]
+        cells = sum(costs[i] for i in mine)
+        g = gather_scores([(i, costs[i]) for i in mine], dist, dst=0)
+        q.put((rank, cells, g))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_fixed_batch_shards_cover_the_batch_on_two_gloo_ranks():
+    """Strong scaling of one 4096-pair batch over two ranks: the ranks' shards are disjoint, their union is the
+    whole batch, and their cells differ by less than the largest pair."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_fixed_shard_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = {}
+    for _ in range(2):
+        rank, cells, g = q.get(timeout=120)
+        out[rank] = (cells, g)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    idx = [i for part in out[0][1] for i, _ in part]
+    assert sorted(idx) == list(range(4096)) and len(set(idx)) == 4096
+    costs = dict((i, c) for part in out[0][1] for i, c in part)
+    assert abs(out[0][0] - out[1][0]) <= max(costs.values())

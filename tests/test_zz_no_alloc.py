@@ -51,6 +51,46 @@ def test_noalloc_matches_regular_entry_point_twice(engine):
         assert got[2] == exp[2]
 
 
+def test_noalloc_against_the_oracle_and_edges(engine, oracle):
+    """The allocation-free call against the CPU oracle: the identity braid of an empty string on either side, and
+    a pair long enough for 32-row lanes (1024-row bands) whose last band is padded."""
+    import torch
+    S = engine
+    for m, n in [(0, 0), (0, 17), (23, 0), (1, 1), (131072 + 500, 3001)]:
+        a, b = gen.uniform_string(m, 4, 23, 1), gen.uniform_string(n, 4, 23, 2)
+        r2c, c2r, score = _run(S, torch, "noalloc", a, b, True)
+        exp = oracle.comb_antidiag(a, b, 8)
+        assert np.array_equal(r2c, exp), (m, n)
+        assert np.array_equal(c2r[exp], np.arange(m + n)), (m, n)
+        assert score == oracle.global_score(exp, m, n), (m, n)
+
+
+def test_noalloc_call_allocates_no_device_memory(engine):
+    """After its first call on the device (which resolves the scratch array's address), a call leaves the free
+    device memory unchanged: nothing is allocated, not even from a pool."""
+    import torch
+    S = engine
+    a, b = gen.uniform_string(70000, 4, 24, 1), gen.uniform_string(5000, 4, 24, 2)
+    m, n = len(a), len(b)
+    da = torch.from_numpy(a).cuda()
+    db = torch.from_numpy(b).cuda()
+    r2c = torch.empty(m + n, dtype=torch.int32, device="cuda")
+    c2r = torch.empty(m + n, dtype=torch.int32, device="cuda")
+    sc = torch.empty(1, dtype=torch.int32, device="cuda")
+    sh = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    L = S.lib()
+    call = lambda: S._lib.check(L.slcs_comb_u8_dev_noalloc(da.data_ptr(), m, db.data_ptr(), n, r2c.data_ptr(),
+                                                           c2r.data_ptr(), sc.data_ptr(), sh))
+    call()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch(engine):
     S = engine
     rc = S.lib().slcs_comb_u8_dev_noalloc(ctypes.c_void_p(1), 9_000_000, ctypes.c_void_p(1), 10, ctypes.c_void_p(1),
