@@ -40,6 +40,8 @@ COMB_DRAM_BYTES_PER_CELL = 3.29e6 / 8.1177e9
 COMB_PIPE_SPLIT = {"alu_pct_of_peak": 80.2, "fma_pct_of_peak": 0.77, "issue_pct": 46.6,
                    "source": "ncu --set full, comb_kernel, 2048-pair batch (profiles/comb_kernel_batch_2048_pairs.md)"}
 SM_COUNT = 148
+# bit-parallel ops per cell: 17 ops per step, 2S - 1 steps per S x S word cell, S = 32 symbols per 64-bit word
+BIT_OPS_PER_CELL = 17 * (2 * 32 - 1) / (32 * 32)
 DIGESTS_PATH = os.path.join(ROOT, "tests", "golden", "headline_digests.json")
 
 
@@ -524,6 +526,18 @@ def run_suite(torch, S, peak_cells, peaks):
             ent["roofline_frac_whole_run"] = round(m * n / (ms * 1e-3) / peak_cells, 4)
             ent["roofline_frac_comb_kernel"] = round(m * n / (kms * 1e-3) / peak_cells, 4)
             braids[name] = r2.cpu().numpy()
+        else:
+            # the bit-parallel convention: 17 ops per step of a 32-symbol word cell, 2S - 1 = 63 steps per
+            # S^2 = 1024 cells (R:prefix_lcs/bitwise/transposition_network_binary_alphabet.h:351-370), against the
+            # SM issue ceiling (one lane-op per issue slot) at the sampled clock
+            ops = BIT_OPS_PER_CELL * m * n
+            ceiling = issue_ceiling_gops({}) * 1e9
+            ent["int_ops_per_cell"] = round(BIT_OPS_PER_CELL, 4)
+            ent["roofline_frac_whole_run"] = round(ops / (ms * 1e-3) / ceiling, 4)
+            ent["roofline_frac_kernel"] = round(ops / (kms * 1e-3) / ceiling, 4)
+            ent["roofline_peak"] = "SM issue ceiling, 148 SM x 4 SMSP x 32 lanes x 1965 MHz"
+            # the same ops against the integer-pipe peak the combing is measured on (probe cells/s x 5 ops)
+            ent["roofline_frac_kernel_vs_probe"] = round(ops / (kms * 1e-3) / (OPS_PER_CELL * peak_cells), 4)
         res[name] = ent
         pl.close()
     res["hybrid_equals_wavefront"] = bool(np.array_equal(braids["hybrid_tiles_4096"], braids["wavefront"]))

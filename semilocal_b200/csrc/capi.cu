@@ -121,7 +121,7 @@ int comb_wavefront_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int3
     SLCS_CUDA_TRY(cudaMemcpyAsync(dpair.p, &hp, sizeof(hp), cudaMemcpyHostToDevice, s));
     SLCS_CUDA_TRY(cudaMemcpyAsync(ditems.p, items.data(), sizeof(CombItem) * items.size(),
                                   cudaMemcpyHostToDevice, s));
-    SLCS_TRY(launch_comb<T>(dpair.p, ditems.p, (int) items.size(), next.p, err.p, comb_resident_warps(E), s));
+    SLCS_TRY(launch_comb_lone<T>(dpair.p, ditems.p, (int) items.size(), next.p, err.p, comb_resident_warps(E), s));
     SLCS_TRY(launch_invert(c2r_work, size, d_r2c, swap, err.p, s));
     if (d_c2r != nullptr && swap) SLCS_TRY(launch_invert(d_r2c, size, d_c2r, false, err.p, s));
     return check_dev_err(err.p, s);

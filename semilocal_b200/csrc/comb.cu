@@ -21,8 +21,17 @@ namespace {
 
 constexpr int kStrandPad = 0x7fffffff;        // strand of a padding column: never smaller than a left strand
 
-template <typename T, int R>
+// One cell: the strands swap iff the symbols match or the left strand's id is larger than the top strand's.
+__device__ __forceinline__ void comb_cell(int A, int bs, int &L, int &t) {
+    const bool sw = (A == bs) | (L > t);
+    const int nt = sw ? L : t;
+    L = sw ? t : L;
+    t = nt;
+}
+
+template <typename T, int R, int CH>
 __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, int *err, int lane) {
+    static_assert(CH == 1 || (CH == 2 && R >= 2), "two chains need at least two rows per lane");
     const T *__restrict__ a = static_cast<const T *>(P.a);
     const T *__restrict__ b = static_cast<const T *>(P.b);
     const int m = P.m, n = P.n;
@@ -44,7 +53,8 @@ __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, 
     const bool has_prev = I.band > 0;
     const int *prev_prog = has_prev ? P.progress + (I.band - 1) : nullptr;
     int *my_prog = P.progress + I.band;
-    const int nchunks = (n + 63) >> 5;   // steps 0 .. n+31 (column n-1 leaves the warp at step n+31)
+    // steps 0 .. n+32*CH-1 (column n-1 leaves the warp's last stage at step n+32*CH-1)
+    const int nchunks = (n + 32 * CH + 31) >> 5;
 
     int io_t = kStrandPad, io_b = kSymColVirtual;
     // Loads the top strands and b-symbols of columns [32q, 32q+32) into io (lane j <- column 32q+j).
@@ -68,7 +78,11 @@ __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, 
     };
 
     if (!load(0)) return;
+    // t / bs: the strand and symbol entering the lane's first row; with two chains (CH = 2) the lane is two
+    // systolic stages, rows [0, R/2) and [R/2, R): tm / bm carry the upper stage's output to the lower stage one
+    // step later, so the two halves work on neighbouring columns at once (two independent dependency chains).
     int t = kStrandPad, bs = kSymColVirtual;
+    int tm = kStrandPad, bm = kSymColVirtual;
     const int src_dn = (lane + 31) & 31, src_up = (lane + 1) & 31;
     for (int q = 0; q < nchunks; ++q) {
 #pragma unroll 4
@@ -83,18 +97,27 @@ __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, 
                 io_t = x;
                 bs = io_b;
             }
+            if (CH == 1) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const bool sw = (A[r] == bs) | (L[r] > t);
-                const int nt = sw ? L[r] : t;
-                L[r] = sw ? t : L[r];
-                t = nt;
+                for (int r = 0; r < R; ++r) comb_cell(A[r], bs, L[r], t);
+            } else {
+                int u = t, w = tm;
+                const int bw = bm;
+#pragma unroll
+                for (int r = 0; r < R / 2; ++r) {
+                    comb_cell(A[r], bs, L[r], u);
+                    comb_cell(A[R / 2 + r], bw, L[R / 2 + r], w);
+                }
+                tm = u;
+                bm = bs;
+                t = w;
+                bs = bw;
             }
             io_t = __shfl_sync(kFull, io_t, src_up);
             io_b = __shfl_sync(kFull, io_b, src_up);
         }
-        // io_t of lane j now holds the strand that left the band's bottom in column 32(q-1)+j.
-        const int col = ((q - 1) << 5) + lane;
+        // io_t of lane j now holds the strand that left the band's bottom in column 32(q-CH)+j.
+        const int col = ((q - CH) << 5) + lane;
         const bool valid = col >= 0 && col < n;
         if (valid) __stcg(P.c2r + col, io_t);
         if (I.last && P.score != nullptr) {
@@ -102,7 +125,7 @@ __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, 
             if (lane == 0 && bal) atomicAdd(P.score, __popc(bal));
         }
         __syncwarp();
-        if (!I.last && lane == 0) st_release(my_prog, min(n, q << 5));
+        if (!I.last && lane == 0 && q >= CH - 1) st_release(my_prog, min(n, (q - CH + 1) << 5));
         if (q + 1 < nchunks && !load(q + 1)) return;
     }
 #pragma unroll
@@ -112,7 +135,10 @@ __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, 
     }
 }
 
-template <typename T>
+// CH = 1: one dependency chain per lane (pairs that share the device with many others: the ALU pipe is the
+// bound, and the shorter pipeline costs 32 fewer steps per band).  CH = 2: two chains per lane, for a lone pair
+// whose bands leave the SMs short of warps, where the chain's latency is the bound.
+template <typename T, int CH>
 __global__ void __launch_bounds__(32, 12) comb_kernel(const CombPair *__restrict__ pairs,
                                                    const CombItem *__restrict__ items, int nitems, int *next,
                                                    int *err) {
@@ -125,12 +151,12 @@ __global__ void __launch_bounds__(32, 12) comb_kernel(const CombPair *__restrict
         const CombItem I = items[it];
         const CombPair P = pairs[I.pair];
         switch (I.R) {
-            case 32: comb_band<T, 32>(P, I, err, lane); break;
-            case 16: comb_band<T, 16>(P, I, err, lane); break;
-            case 8: comb_band<T, 8>(P, I, err, lane); break;
-            case 4: comb_band<T, 4>(P, I, err, lane); break;
-            case 2: comb_band<T, 2>(P, I, err, lane); break;
-            default: comb_band<T, 1>(P, I, err, lane); break;
+            case 32: comb_band<T, 32, CH>(P, I, err, lane); break;
+            case 16: comb_band<T, 16, CH>(P, I, err, lane); break;
+            case 8: comb_band<T, 8, CH>(P, I, err, lane); break;
+            case 4: comb_band<T, 4, CH>(P, I, err, lane); break;
+            case 2: comb_band<T, 2, CH>(P, I, err, lane); break;
+            default: comb_band<T, 1, 1>(P, I, err, lane); break;
         }
     }
 }
@@ -180,16 +206,28 @@ int launch_comb(const CombPair *d_pairs, const CombItem *d_items, int nitems, in
     if (nitems <= 0) return SLCS_OK;
     // one warp per block (the warps are independent workers), so that few items still spread over all SMs
     const int warps = grid_warps < nitems ? grid_warps : nitems;
-    comb_kernel<T><<<warps, 32, 0, s>>>(d_pairs, d_items, nitems, d_next, d_err);
+    comb_kernel<T, 1><<<warps, 32, 0, s>>>(d_pairs, d_items, nitems, d_next, d_err);
     SLCS_CUDA_TRY(cudaGetLastError());
     return SLCS_OK;
 }
 template int launch_comb<uint8_t>(const CombPair *, const CombItem *, int, int *, int *, int, cudaStream_t);
 template int launch_comb<int32_t>(const CombPair *, const CombItem *, int, int *, int *, int, cudaStream_t);
 
+template <typename T>
+int launch_comb_lone(const CombPair *d_pairs, const CombItem *d_items, int nitems, int *d_next, int *d_err,
+                     int grid_warps, cudaStream_t s) {
+    if (nitems <= 0) return SLCS_OK;
+    const int warps = grid_warps < nitems ? grid_warps : nitems;
+    comb_kernel<T, 2><<<warps, 32, 0, s>>>(d_pairs, d_items, nitems, d_next, d_err);
+    SLCS_CUDA_TRY(cudaGetLastError());
+    return SLCS_OK;
+}
+template int launch_comb_lone<uint8_t>(const CombPair *, const CombItem *, int, int *, int *, int, cudaStream_t);
+template int launch_comb_lone<int32_t>(const CombPair *, const CombItem *, int, int *, int *, int, cudaStream_t);
+
 int comb_resident_warps_sm(int num_sms) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, comb_kernel<uint8_t>, 32, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, comb_kernel<uint8_t, 1>, 32, 0) != cudaSuccess ||
         per_sm <= 0) {
         cudaGetLastError();
         per_sm = 12;

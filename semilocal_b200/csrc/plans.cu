@@ -49,7 +49,8 @@ int wave_run(slcs_pair_plan *P, const uint8_t *d_a, const uint8_t *d_b, int32_t 
     if (d_score) SLCS_CUDA_TRY(cudaMemsetAsync(d_score, 0, sizeof(int32_t), s));
     const unsigned fl = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     SLCS_CUDA_TRY(cudaEventRecordWithFlags(P->ev0, s, fl));
-    SLCS_TRY(launch_comb<uint8_t>(P->d_pair, P->d_items, (int) P->items.size(), P->d_next, P->d_err, P->resident, s));
+    SLCS_TRY(launch_comb_lone<uint8_t>(P->d_pair, P->d_items, (int) P->items.size(), P->d_next, P->d_err,
+                                       P->resident, s));
     SLCS_CUDA_TRY(cudaEventRecordWithFlags(P->ev1, s, fl));
     SLCS_TRY(launch_invert(P->d_c2r, P->m + P->n, d_r2c, false, P->d_err, s));
     return SLCS_OK;

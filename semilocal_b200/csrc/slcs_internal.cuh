@@ -174,6 +174,10 @@ int plan_bands(int pair, int m, int R, std::vector<CombItem> &items);
 template <typename T>
 int launch_comb(const CombPair *d_pairs, const CombItem *d_items, int nitems, int *d_next, int *d_err,
                 int grid_warps, cudaStream_t s);
+// The same for the bands of one pair alone on the device: two dependency chains per lane (comb.cu).
+template <typename T>
+int launch_comb_lone(const CombPair *d_pairs, const CombItem *d_items, int nitems, int *d_next, int *d_err,
+                     int grid_warps, cudaStream_t s);
 // Warps that fit on the device at once for the combing kernel.
 int comb_resident_warps(Engine *E);
 int comb_resident_warps_sm(int num_sms);
