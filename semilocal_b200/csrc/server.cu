@@ -275,7 +275,7 @@ void finish_req(slcs_server *S, Req *r, int status, int32_t score, double t_done
 }
 
 // Builds and enqueues one launch of the requests on stream idx.  Their budget is already reserved.
-int launch_group(slcs_server *S, int idx, std::vector<Req *> &reqs, int warp_cap) {
+int launch_group(slcs_server *S, int idx, std::vector<Req *> &reqs, int warp_cap, bool lone = false) {
     NvtxRange nv("slcs: server launch");
     cudaStream_t s = S->streams[idx];
     std::sort(reqs.begin(), reqs.end(), [](const Req *x, const Req *y) { return x->cells > y->cells; });
@@ -347,9 +347,10 @@ int launch_group(slcs_server *S, int idx, std::vector<Req *> &reqs, int warp_cap
         cudaMemsetAsync(D + o_out, 0, bytes - o_out, s) != cudaSuccess)
         return fail_all(fail(SLCS_ERR_CUDA, "launch metadata upload failed"));
     int *derr = reinterpret_cast<int *>(D + o_err);
-    int rc = launch_comb<uint8_t>(reinterpret_cast<const CombPair *>(D + o_pairs),
-                                  reinterpret_cast<const CombItem *>(D + o_items), ni, derr + 1, derr,
-                                  std::max(1, warp_cap), s);
+    // a launch of one big request that has the device to itself combs with two dependency chains per lane
+    int rc = (lone ? launch_comb_lone<uint8_t> : launch_comb<uint8_t>)(
+        reinterpret_cast<const CombPair *>(D + o_pairs), reinterpret_cast<const CombItem *>(D + o_items), ni,
+        derr + 1, derr, std::max(1, warp_cap), s);
     if (rc != SLCS_OK) return fail_all(rc);
     int maxsize = 1;
     for (Req *r : reqs) maxsize = std::max(maxsize, r->m + r->n);
@@ -459,7 +460,14 @@ bool schedule(slcs_server *S) {
         }
         if (g.empty()) break;
         pending_big -= (int) g.size();
-        launch_group(S, idx, g, S->o.big_warps > 0 ? S->o.big_warps : W / 2);
+        // the grid cap: half the resident warps while big launches may overlap; when this launch is the only
+        // big work (one request on an otherwise idle big side, nothing big pending) three quarters of them and
+        // two chains per lane, since a 1M-row request has ~1000 bands and a half grid would run its later bands
+        // only after whole earlier ones.  A quarter always stays free for a small batch.
+        bool alone = g.size() == 1 && pending_big == 0;
+        for (int j = 0; j < S->nbig && alone; ++j) alone = j == idx || S->inflight[j] == nullptr;
+        const int cap = S->o.big_warps > 0 ? S->o.big_warps : (alone ? W - W / 4 : W / 2);
+        launch_group(S, idx, g, cap, alone);
         did = true;
     }
     // small streams: everything small that fits, oldest first, up to max_batch per launch
