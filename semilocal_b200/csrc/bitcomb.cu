@@ -34,14 +34,13 @@ struct BitPair {
     int32_t *progress;              // per band: number of hand-off words written
     int32_t *ones;                  // out: popcount of the final left strands over real rows
     int m, n, nstrips, nblocks;
-    int chunk;                      // hand-off words published / polled together (1..32)
 };
 
 struct BitItem {
     int pair, band, s0, last;
 };
 
-constexpr int kChunkDefault = 16;   // hand-off words between bands are published / polled in groups of this size
+constexpr int kChunk = 16;   // hand-off words between bands are published / polled in groups of kChunk
 
 // One band (warp).  Lane k owns strips s0 + k RS + r, r = 0..RS-1.  The strips of a lane form one systolic
 // chain: strip r works one 32-step block behind strip r-1 and takes its input bit, each step, straight from
@@ -70,7 +69,7 @@ __device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int
     const int lag = lane * (RS + 1);
     const int gmax = 31 * (RS + 1) + RS - 1 + nb;
     uint32_t carry = 0u;    // input word of strip 0, from the lane above (previous iteration)
-    uint32_t chunkw = 0u;   // lanes 0..chunk-1: the current chunk of hand-off words from the band above
+    uint32_t chunkw = 0u;   // lanes 0..kChunk-1: the current chunk of hand-off words from the band above
     // Column-plane words (index 0 .. nb + 2) reach the lanes through a ring in shared memory: the warp loads
     // 32 words per plane every 32 iterations, 64 words ahead, and stores them one iteration later, so no load
     // latency sits on the loop.  At iteration g the lanes read words >= g - 31 (RS + 1) - RS + 1 and <= g + 3;
@@ -114,16 +113,15 @@ __device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int
             }
         }
         // lane 0's input word: from the band above (zero strands for the first band).  The band above is
-        // polled once per chunk of words; the chunk's words are then loaded by lanes 0..chunk-1 in one go and
+        // polled once per kChunk words; the chunk's words are then loaded by lanes 0..kChunk-1 in one go and
         // handed to lane 0 by shuffle, one per iteration.
-        const int gc = g % P.chunk;
-        if (I.band > 0 && g < nb && gc == 0) {
+        if (I.band > 0 && g < nb && (g % kChunk) == 0) {
             int ok = 1;
-            if (lane == 0) ok = wait_at_least(P.progress + (I.band - 1), min(nb, g + P.chunk), err) ? 1 : 0;
+            if (lane == 0) ok = wait_at_least(P.progress + (I.band - 1), min(nb, g + kChunk), err) ? 1 : 0;
             if (!__shfl_sync(kFull, ok, 0)) return;   // the bounded wait gave up (error word set)
-            chunkw = (lane < P.chunk && g + lane < nb) ? __ldcg(P.hand + g + lane) : 0u;
+            chunkw = (lane < kChunk && g + lane < nb) ? __ldcg(P.hand + g + lane) : 0u;
         }
-        const uint32_t hw = __shfl_sync(kFull, chunkw, gc);
+        const uint32_t hw = __shfl_sync(kFull, chunkw, g % kChunk);
         uint32_t io = lane == 0 ? ((I.band > 0 && g < nb) ? hw : 0u) : carry;
         // column-plane words of every strip's block (loaded one iteration ahead; q clamped to [-1, nb]:
         // words q - 1 and q sit at indices q + 1, q + 2 in [0, nb + 2])
@@ -166,8 +164,8 @@ __device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int
         const int w = g - lag - RS;
         if (lane == 31 && !I.last && w >= 0 && w < nb) {
             __stcg(P.hand + w, out);
-            // publish once per chunk of words; the release store orders this lane's earlier stores before it
-            if ((w + 1) % P.chunk == 0 || w + 1 == nb) st_release(P.progress + I.band, w + 1);
+            // publish once per kChunk words; the release store orders this lane's earlier stores before it
+            if ((w + 1) % kChunk == 0 || w + 1 == nb) st_release(P.progress + I.band, w + 1);
         }
         carry = __shfl_up_sync(kFull, out, 1);
     }
@@ -228,15 +226,6 @@ __global__ void bit_pack_kernel(const uint8_t *__restrict__ a, int m, const uint
             }
         }
     }
-}
-
-int handoff_chunk() {
-    // tuning override of the hand-off granularity (1..32 words), e.g. for the autotuner
-    if (const char *env = getenv("SLCS_BIT_HANDOFF_WORDS")) {
-        const int v = atoi(env);
-        if (v >= 1 && v <= 32) return v;
-    }
-    return kChunkDefault;
 }
 
 int strips_per_lane(int nstrips) {
@@ -309,8 +298,7 @@ int bit_plan_create(Engine *E, int m, int n, cudaStream_t s, BitPlan **out) {
     BP_ALLOC(dp, 1);
     BP_ALLOC(di, B->bands);
 #undef BP_ALLOC
-    BitPair hp{B->a1, B->a0, B->b1, B->b0, B->b2, B->hand, B->prog, B->ones, m, n, B->nstrips, B->nblocks,
-               handoff_chunk()};
+    BitPair hp{B->a1, B->a0, B->b1, B->b0, B->b2, B->hand, B->prog, B->ones, m, n, B->nstrips, B->nblocks};
     std::vector<BitItem> items(B->bands);
     for (int b = 0; b < B->bands; ++b) items[b] = BitItem{0, b, b * per_band, b == B->bands - 1 ? 1 : 0};
     if (cudaMemcpyAsync(B->dp, &hp, sizeof(hp), cudaMemcpyHostToDevice, s) != cudaSuccess ||

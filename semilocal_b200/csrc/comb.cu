@@ -22,15 +22,22 @@ namespace {
 constexpr int kStrandPad = 0x7fffffff;        // strand of a padding column: never smaller than a left strand
 
 // One cell: the strands swap iff the symbols match or the left strand's id is larger than the top strand's.
-__device__ __forceinline__ void comb_cell(int A, int bs, int &L, int &t) {
+// The two strands leave the cell as they entered it, possibly swapped, so the left strand's new id is
+// (L + t) - nt.  That sum and difference are two IMADs with multipliers `one` = 1 and `neg1` = -1 passed in as
+// kernel parameters (the compiler cannot fold them into additions), which run on the FMA pipe; the compares and
+// the select stay on the ALU pipe.  Three ALU ops per cell instead of four (two compares, two selects): the ALU
+// pipe is the bound at full occupancy, and the FMA pipe is otherwise idle.
+__device__ __forceinline__ void comb_cell(int A, int bs, int &L, int &t, int one, int neg1) {
+    const int sum = L * one + t;
     const bool sw = (A == bs) | (L > t);
     const int nt = sw ? L : t;
-    L = sw ? t : L;
+    L = nt * neg1 + sum;
     t = nt;
 }
 
 template <typename T, int R, int CH>
-__device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, int *err, int lane) {
+__device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, int *err, int lane, int one,
+                                          int neg1) {
     static_assert(CH == 1 || (CH == 2 && R >= 2), "two chains need at least two rows per lane");
     const T *__restrict__ a = static_cast<const T *>(P.a);
     const T *__restrict__ b = static_cast<const T *>(P.b);
@@ -99,14 +106,14 @@ __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, 
             }
             if (CH == 1) {
 #pragma unroll
-                for (int r = 0; r < R; ++r) comb_cell(A[r], bs, L[r], t);
+                for (int r = 0; r < R; ++r) comb_cell(A[r], bs, L[r], t, one, neg1);
             } else {
                 int u = t, w = tm;
                 const int bw = bm;
 #pragma unroll
                 for (int r = 0; r < R / 2; ++r) {
-                    comb_cell(A[r], bs, L[r], u);
-                    comb_cell(A[R / 2 + r], bw, L[R / 2 + r], w);
+                    comb_cell(A[r], bs, L[r], u, one, neg1);
+                    comb_cell(A[R / 2 + r], bw, L[R / 2 + r], w, one, neg1);
                 }
                 tm = u;
                 bm = bs;
@@ -137,11 +144,11 @@ __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, 
 
 // CH = 1: one dependency chain per lane (pairs that share the device with many others: the ALU pipe is the
 // bound, and the shorter pipeline costs 32 fewer steps per band).  CH = 2: two chains per lane, for a lone pair
-// whose bands leave the SMs short of warps, where the chain's latency is the bound.
+// whose few bands leave the SMs short of warps, where the chain's latency is the bound.  one = 1, neg1 = -1.
 template <typename T, int CH>
 __global__ void __launch_bounds__(32, 12) comb_kernel(const CombPair *__restrict__ pairs,
                                                    const CombItem *__restrict__ items, int nitems, int *next,
-                                                   int *err) {
+                                                   int *err, int one, int neg1) {
     const int lane = threadIdx.x & 31;
     for (;;) {
         int it = nitems;
@@ -151,12 +158,12 @@ __global__ void __launch_bounds__(32, 12) comb_kernel(const CombPair *__restrict
         const CombItem I = items[it];
         const CombPair P = pairs[I.pair];
         switch (I.R) {
-            case 32: comb_band<T, 32, CH>(P, I, err, lane); break;
-            case 16: comb_band<T, 16, CH>(P, I, err, lane); break;
-            case 8: comb_band<T, 8, CH>(P, I, err, lane); break;
-            case 4: comb_band<T, 4, CH>(P, I, err, lane); break;
-            case 2: comb_band<T, 2, CH>(P, I, err, lane); break;
-            default: comb_band<T, 1, 1>(P, I, err, lane); break;
+            case 32: comb_band<T, 32, CH>(P, I, err, lane, one, neg1); break;
+            case 16: comb_band<T, 16, CH>(P, I, err, lane, one, neg1); break;
+            case 8: comb_band<T, 8, CH>(P, I, err, lane, one, neg1); break;
+            case 4: comb_band<T, 4, CH>(P, I, err, lane, one, neg1); break;
+            case 2: comb_band<T, 2, CH>(P, I, err, lane, one, neg1); break;
+            default: comb_band<T, 1, 1>(P, I, err, lane, one, neg1); break;
         }
     }
 }
@@ -206,7 +213,7 @@ int launch_comb(const CombPair *d_pairs, const CombItem *d_items, int nitems, in
     if (nitems <= 0) return SLCS_OK;
     // one warp per block (the warps are independent workers), so that few items still spread over all SMs
     const int warps = grid_warps < nitems ? grid_warps : nitems;
-    comb_kernel<T, 1><<<warps, 32, 0, s>>>(d_pairs, d_items, nitems, d_next, d_err);
+    comb_kernel<T, 1><<<warps, 32, 0, s>>>(d_pairs, d_items, nitems, d_next, d_err, 1, -1);
     SLCS_CUDA_TRY(cudaGetLastError());
     return SLCS_OK;
 }
@@ -218,7 +225,12 @@ int launch_comb_lone(const CombPair *d_pairs, const CombItem *d_items, int nitem
                      int grid_warps, cudaStream_t s) {
     if (nitems <= 0) return SLCS_OK;
     const int warps = grid_warps < nitems ? grid_warps : nitems;
-    comb_kernel<T, 2><<<warps, 32, 0, s>>>(d_pairs, d_items, nitems, d_next, d_err);
+    // two chains per lane only while the bands fill at most half the resident warps (measured on B200: 8192^2,
+    // up to 256 bands, 1.09 -> 0.92 ms; the 2^20 pair's 1024 bands gain nothing from it)
+    if (2 * nitems <= grid_warps)
+        comb_kernel<T, 2><<<warps, 32, 0, s>>>(d_pairs, d_items, nitems, d_next, d_err, 1, -1);
+    else
+        comb_kernel<T, 1><<<warps, 32, 0, s>>>(d_pairs, d_items, nitems, d_next, d_err, 1, -1);
     SLCS_CUDA_TRY(cudaGetLastError());
     return SLCS_OK;
 }

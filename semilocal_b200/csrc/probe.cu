@@ -1,16 +1,17 @@
 // probe.cu -- measured ceiling of the combing cell's instruction mix (the integer-pipe roofline).
 //
 // Every thread runs 8 independent combing cells per iteration (distinct a-symbols, independent strand
-// pairs), i.e. the cell rule of comb.cu without its data dependencies, shuffles or memory traffic.  The
-// resulting cells/s, at full occupancy, is the issue-rate ceiling that the combing kernels are measured
-// against ("roofline.peak"); 5 integer ops per cell is the reporting convention (compare, compare, or,
-// two selects).
+// pairs), i.e. the cell of comb.cu -- two compares and a select on the ALU pipe, the left strand's new id as
+// (L + t) - nt by two IMADs on the FMA pipe -- without its data dependencies, shuffles or memory traffic.  The
+// resulting cells/s, at full occupancy, is the ceiling of that instruction mix that the combing kernels are
+// measured against ("roofline.peak"); 5 integer ops per cell is the reporting convention (compare, compare,
+// or, two selects).
 #include "slcs_internal.cuh"
 
 namespace slcs {
 namespace {
 
-__global__ void __launch_bounds__(256) probe_cells_kernel(int iters, int seed, int *out) {
+__global__ void __launch_bounds__(256) probe_cells_kernel(int iters, int seed, int *out, int one, int neg1) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     int L[8], t[8], A[8];
 #pragma unroll
@@ -23,9 +24,10 @@ __global__ void __launch_bounds__(256) probe_cells_kernel(int iters, int seed, i
     for (int i = 0; i < iters; ++i) {
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
+            const int sum = L[k] * one + t[k];
             const bool sw = (A[k] == bs) | (L[k] > t[k]);
             const int nt = sw ? L[k] : t[k];
-            L[k] = sw ? t[k] : L[k];
+            L[k] = nt * neg1 + sum;
             t[k] = nt;
         }
         bs = t[i & 7] & 3;
@@ -55,11 +57,11 @@ extern "C" int slcs_probe_cell_peak(double *cells_per_sec) {
     cudaEvent_t e0, e1;
     SLCS_CUDA_TRY(cudaEventCreate(&e0));
     SLCS_CUDA_TRY(cudaEventCreate(&e1));
-    probe_cells_kernel<<<blocks, 256, 0, s>>>(iters, 1, out.p);   // warm-up
+    probe_cells_kernel<<<blocks, 256, 0, s>>>(iters, 1, out.p, 1, -1);   // warm-up
     float best = 1e30f;
     for (int rep = 0; rep < 5; ++rep) {
         SLCS_CUDA_TRY(cudaEventRecord(e0, s));
-        probe_cells_kernel<<<blocks, 256, 0, s>>>(iters, rep, out.p);
+        probe_cells_kernel<<<blocks, 256, 0, s>>>(iters, rep, out.p, 1, -1);
         SLCS_CUDA_TRY(cudaEventRecord(e1, s));
         SLCS_CUDA_TRY(cudaEventSynchronize(e1));
         float ms = 0;
