@@ -435,6 +435,9 @@ bool retire(slcs_server *S) {
     return did;
 }
 
+// Cells per second a request is assumed to comb at when the scheduler orders big requests (B200, batched rate).
+constexpr double kServeCellsPerSec = 5.0e12;
+
 bool schedule(slcs_server *S) {
     bool did = false;
     const int W = S->resident_warps;
@@ -448,15 +451,23 @@ bool schedule(slcs_server *S) {
         int free_big = 0;
         for (int j = idx; j < S->nbig; ++j) free_big += S->inflight[j] == nullptr;
         const int share = std::min(8, std::max(1, (pending_big + free_big - 1) / free_big));
+        // which big requests first: the least remaining time, i.e. the request's own combing time (at the
+        // device's batched rate) minus the time it has already waited -- short requests overtake long ones, and a
+        // long one that has waited as long as its own work takes goes first (so none starves)
+        const double now = S->now();
+        std::vector<std::pair<double, Req *>> cand;
+        for (Req *r : S->pending)
+            if (big(r)) cand.emplace_back((double) r->cells / kServeCellsPerSec - (now - r->t_submit), r);
+        std::stable_sort(cand.begin(), cand.end(),
+                         [](const std::pair<double, Req *> &x, const std::pair<double, Req *> &y) {
+                             return x.first < y.first;
+                         });
         std::vector<Req *> g;
-        for (auto it = S->pending.begin(); it != S->pending.end() && (int) g.size() < share;) {
-            if (!big(*it)) {
-                ++it;
-                continue;
-            }
-            if (!reserve(S, (*it)->need, S->streams[idx])) break;
-            g.push_back(*it);
-            it = S->pending.erase(it);
+        for (const auto &c : cand) {
+            if ((int) g.size() >= share) break;
+            if (!reserve(S, c.second->need, S->streams[idx])) break;
+            g.push_back(c.second);
+            S->pending.erase(std::find(S->pending.begin(), S->pending.end(), c.second));
         }
         if (g.empty()) break;
         pending_big -= (int) g.size();
