@@ -36,8 +36,8 @@ OPS_PER_CELL = 5     # compare, compare, or, two selects (R:include/SemiLocal/Se
 # its bands x columns, i.e. with its cells at a fixed band height, so the bench scales it by cells.
 COMB_DRAM_BYTES_PER_CELL = 3.29e6 / 8.1177e9
 # Pipe split of comb_kernel from ncu (profiles/comb_kernel_batch_2048_pairs.md): the ALU pipe carries the cell's
-# compares and selects, the FMA pipe is idle; the issue slots are half used.
-COMB_PIPE_SPLIT = {"alu_pct_of_peak": 80.2, "fma_pct_of_peak": 0.77, "issue_pct": 46.6,
+# compares and select, the FMA pipe its two IMADs; the issue slots are two-thirds used.
+COMB_PIPE_SPLIT = {"alu_pct_of_peak": 60.6, "fma_pct_of_peak": 31.6, "issue_pct": 69.3,
                    "source": "ncu --set full, comb_kernel, 2048-pair batch (profiles/comb_kernel_batch_2048_pairs.md)"}
 SM_COUNT = 148
 # bit-parallel ops per cell: 17 ops per step, 2S - 1 steps per S x S word cell, S = 32 symbols per 64-bit word
