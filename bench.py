@@ -31,10 +31,10 @@ from semilocal_b200.shard import max_over_ranks, shard_pairs  # noqa: E402
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 OPS_PER_CELL = 5     # compare, compare, or, two selects (R:include/SemiLocal/SemiLocalLCS.h:158-172)
-# DRAM bytes (read + write) per cell of comb_kernel, from one ncu capture of the 256-pair batch case
-# (`python -m semilocal_b200.profile_cases batch 256`: 3.29 MB for 8.12e9 cells); a launch's traffic grows with
-# its bands x columns, i.e. with its cells at a fixed band height, so the bench scales it by cells.
-COMB_DRAM_BYTES_PER_CELL = 3.29e6 / 8.1177e9
+# DRAM bytes (read + write) per cell of comb_kernel, from one ncu capture of the 2048-pair batch case
+# (`python -m semilocal_b200.profile_cases batch 2048`: 16.68 + 10.24 MB for 6.5112e10 cells); a launch's traffic grows
+# with its bands x columns, i.e. with its cells at a fixed band height, so the bench scales it by cells.
+COMB_DRAM_BYTES_PER_CELL = 26.925e6 / 6.5112e10
 # Pipe split of comb_kernel from ncu (profiles/comb_kernel_batch_2048_pairs.md): the ALU pipe carries the cell's
 # compares and select, the FMA pipe its two IMADs; the issue slots are two-thirds used.
 COMB_PIPE_SPLIT = {"alu_pct_of_peak": 60.6, "fma_pct_of_peak": 31.6, "issue_pct": 69.3,
@@ -382,7 +382,7 @@ def run_ours(args, rank, world, local):
                      "unit": "Gop/s", "frac": round(achieved_gops / peak_gops, 4),
                      "traffic": int(COMB_DRAM_BYTES_PER_CELL * cells),
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of comb_kernel on the "
-                                       "256-pair batch case, scaled to this launch by cells",
+                                       "2048-pair batch case, scaled to this launch by cells",
                      "kernel": "comb_kernel", "kernel_ms": round(k_ms, 3),
                      "kernel_ms_source": f"mean of {len(kern_ms)} graph replays' kernel events",
                      "peak_source": "slcs_probe_cell_peak (cell instruction mix, full occupancy), x5 ops/cell",
