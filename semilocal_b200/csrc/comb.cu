@@ -62,8 +62,11 @@ __device__ __forceinline__ void st_release_block(int *p, int v) {
 __device__ __forceinline__ bool wait_block_at_least(const int *p, int need, int *err) {
     if (ld_acquire_block(p) >= need) return true;
     const unsigned long long t0 = global_ns();
+    // a band waits for the band above it in the same CTA, which runs one chunk ahead: spin on the shared counter
+    // (no sleep, whose granularity would be added to every hand-off), checking the error word and the clock
+    // every 64 polls, and only after 2^14 polls sleep between polls
     for (long long it = 0; it < (1ll << 28); ++it) {
-        __nanosleep(32);
+        if (it >= (1 << 14)) __nanosleep(32);
         if (ld_acquire_block(p) >= need) return true;
         if ((it & 63) == 63) {
             if (ld_relaxed(err) != kDevErrNone) return false;

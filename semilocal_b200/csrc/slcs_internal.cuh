@@ -27,6 +27,7 @@ constexpr int kDevErrBadState = 2;    // an internal consistency check failed
 // waits (a band waiting for the band above it to publish 32 columns) last microseconds.
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 constexpr unsigned kSpinSleepNs = 100;
+constexpr int kSpinPolls = 64;   // polls without sleeping before the sleeping ones
 
 // NVTX range for the host side of a stage (visible in Nsight timelines; no cost without a tool attached).
 struct NvtxRange {
@@ -86,8 +87,14 @@ __device__ __forceinline__ bool wait_at_least(const int *p, int need, int *err,
                                               unsigned long long limit_ns = kWaitLimitNs) {
     if (ld_acquire(p) >= need) return true;
     const unsigned long long t0 = global_ns();
-    // the iteration cap is a second bound in case the timer does not advance (at >= 100 ns per poll it is
-    // never the first to trigger while the timer runs)
+    // the first polls follow each other without sleeping (a band usually waits for the band above to publish
+    // its next chunk, well under a microsecond; a sleep there would add its own granularity to every hand-off);
+    // then one poll every ~kSpinSleepNs.  The iteration cap is a second bound in case the timer does not advance
+    // (at >= 100 ns per poll it is never the first to trigger while the timer runs).
+#pragma unroll 1
+    for (int it = 0; it < kSpinPolls; ++it) {
+        if (ld_acquire(p) >= need) return true;
+    }
     for (long long it = 0; it < (1ll << 26); ++it) {
         __nanosleep(kSpinSleepNs);
         if (ld_acquire(p) >= need) return true;
