@@ -189,7 +189,8 @@ __global__ void __launch_bounds__(32) bit_kernel(const BitPair *__restrict__ pai
         it = __shfl_sync(kFull, it, 0);
         if (it >= nitems) return;
         const BitItem I = items[it];
-        bit_band<RS>(pairs[I.pair], I, err, lane, ring);
+        const BitPair P = pairs[I.pair];   // by value: no field reloads after the loop's global stores
+        bit_band<RS>(P, I, err, lane, ring);
     }
 }
 

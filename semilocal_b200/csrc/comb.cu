@@ -111,9 +111,14 @@ __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, 
     const int nchunks = (n + 32 * CH + 31) >> 5;
 
     int io_t = kStrandPad, io_b = kSymColVirtual;
+    // b-symbols are read one chunk ahead of their use (they do not depend on the band above), so the load's
+    // latency is not exposed at every chunk boundary of a band that has the SM to itself
+    int pre_b = lane < n ? static_cast<int>(b[lane]) : kSymColVirtual;
     // Loads the top strands and b-symbols of columns [32q, 32q+32) into io (lane j <- column 32q+j).
     auto load = [&](int q) -> bool {
         const int c0 = q << 5;
+        io_b = pre_b;
+        pre_b = c0 + 32 + lane < n ? static_cast<int>(b[c0 + 32 + lane]) : kSymColVirtual;
         if (CTA && in_s) {
             const int c = c0 + lane;
             if (c0 < n) {
@@ -127,7 +132,6 @@ __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, 
             } else {
                 io_t = kStrandPad;
             }
-            io_b = c < n ? static_cast<int>(b[c]) : kSymColVirtual;
             return true;
         }
         if (has_prev && c0 < n) {
@@ -137,13 +141,7 @@ __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, 
             if (!ok) return false;
         }
         const int c = c0 + lane;
-        if (c < n) {
-            io_t = has_prev ? __ldcg(P.c2r + c) : (m + c);
-            io_b = static_cast<int>(b[c]);
-        } else {
-            io_t = kStrandPad;
-            io_b = kSymColVirtual;
-        }
+        io_t = c < n ? (has_prev ? __ldcg(P.c2r + c) : (m + c)) : kStrandPad;
         return true;
     };
 
