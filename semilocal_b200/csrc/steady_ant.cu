@@ -359,17 +359,24 @@ __device__ __forceinline__ void warp_low_levels(SaShared &S, int o, const int (&
         }
         // c*(r) = min{c : delta(r, c) >= 0}, delta(r, 0) = -#{lo points in rows >= r}
         const int r = lane - a;
-        unsigned mine[NG];   // bit g: colind(g, r) for the columns g of the lane's node, row r = lane - a
+        // mine: bit g (warp lane of column g) = colind(g, r) for the columns of the lane's node, row r = lane - a.
+        // In row 0 the set is the node's lo columns (a lo column counts while r <= its point's row, a hi column
+        // once r is past it); going down one row flips exactly the column of the row's point.  So the set of row r
+        // is the lo columns XOR the points' columns of the rows above r: one ballot and a segmented prefix XOR
+        // over the node's lanes (log2 s shuffles) instead of one ballot per row.
+        unsigned mine[NG];
 #pragma unroll
-        for (int j = 0; j < NG; ++j) mine[j] = 0u;
+        for (int j = 0; j < NG; ++j) {
+            const unsigned lo_cols = __ballot_sync(kFull, two[j] && !(y[j] >> 15));
+            const unsigned own = two[j] ? (1u << (a + (x[j] & 0x7fff))) : 0u;
+            unsigned v = own;
 #pragma unroll
-        for (int i = 0; i < s; ++i) {
-#pragma unroll
-            for (int j = 0; j < NG; ++j) {
-                const int yr = y[j] & 0x7fff;
-                const unsigned M = __ballot_sync(kFull, two[j] && ((y[j] >> 15) ? (yr < i) : (yr >= i)));
-                if (r == i) mine[j] = M;
+            for (int d = 1; d < 32; d <<= 1) {
+                if (d >= s) break;
+                const unsigned t = __shfl_up_sync(kFull, v, d);
+                if (r >= d) v ^= t;
             }
+            mine[j] = lo_cols ^ (v ^ own);
         }
 #pragma unroll
         for (int j = 0; j < NG; ++j) {
