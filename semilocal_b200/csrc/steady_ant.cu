@@ -1120,14 +1120,30 @@ __device__ __forceinline__ int band_row_count(const int32_t *X, int i0, int i1, 
     });
 }
 
+// warp-wide: as ballot_search, but the first 32 candidates are tried alone and the rest 256 at a time: most
+// searches end within a few columns, while a long one (a band whose column range spans a large part of the node,
+// as in the glue of the braids of two similar strings, read from global memory) then costs an eighth of the rounds
+template <typename Pred>
+__device__ __forceinline__ int ballot_search_grow(int from, int end, int need, int none, int lane, Pred pred) {
+    if (need <= 0) return from;
+    const int g = from + lane;
+    const unsigned m = __ballot_sync(kFull, g < end && pred(g));
+    const int cnt = __popc(m);
+    if (need <= cnt) return from + (int) __fns(m, 0, need) + 1;
+    return ballot_search<8>(from + 32, end, need - cnt, none, lane, pred);
+}
+
 // warp-wide: one past the need-th column g in [from, cend) whose point raises delta in row R; k + 1 if none
-template <int U = 1>
+// (U = 0: the growing search above)
+template <int U = 0>
 __device__ __forceinline__ int band_col_search(const YView &Y, int k, int from, int cend, int need, int R, int lane) {
-    return ballot_search<U>(from, cend, need, k + 1, lane, [&](int g) {
+    auto pred = [&](int g) {
         const int w = Y(g);
         const int y = w & kValMask;
         return (w & kHiBit) ? (y < R) : (y >= R);
-    });
+    };
+    if constexpr (U == 0) return ballot_search_grow(from, cend, need, k + 1, lane, pred);
+    else return ballot_search<U>(from, cend, need, k + 1, lane, pred);
 }
 
 // one thread: band rows [i0, i1) walked up from c = c*(R0 + i1)
