@@ -509,9 +509,11 @@ def run_suite(torch, S, peak_cells, peaks):
     da, db = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
     res = {}
     braids = {}
-    for name, kind in (("hybrid_tiles_4096", S.ALGO_HYBRID), ("wavefront", S.ALGO_WAVEFRONT),
-                       ("bit_parallel", S.PLAN_BITPARALLEL)):
-        pl = S.PairPlan(m, n, kind, tile=4096 if kind == S.ALGO_HYBRID else 0)
+    # the hybrid with the configuration's 4096 x 4096 tiles, and with 65536 x 65536 tiles (the reference's own
+    # OpenMPHybridIterative(threads, 65536, 65536): 256 tiles, 8 glue levels instead of 16)
+    for name, kind, tile in (("hybrid_tiles_4096", S.ALGO_HYBRID, 4096), ("hybrid_tiles_65536", S.ALGO_HYBRID, 65536),
+                             ("wavefront", S.ALGO_WAVEFRONT, 0), ("bit_parallel", S.PLAN_BITPARALLEL, 0)):
+        pl = S.PairPlan(m, n, kind, tile=tile)
         r2 = torch.empty(m + n, dtype=torch.int32, device="cuda") if kind != S.PLAN_BITPARALLEL else None
         sc2 = torch.zeros(1, dtype=torch.int32, device="cuda")
         fn = lambda: pl.run(da.data_ptr(), db.data_ptr(), r2.data_ptr() if r2 is not None else None,
@@ -540,8 +542,10 @@ def run_suite(torch, S, peak_cells, peaks):
             ent["roofline_frac_kernel_vs_probe"] = round(ops / (kms * 1e-3) / (OPS_PER_CELL * peak_cells), 4)
         res[name] = ent
         pl.close()
-    res["hybrid_equals_wavefront"] = bool(np.array_equal(braids["hybrid_tiles_4096"], braids["wavefront"]))
-    res["scores_agree"] = len({res[k]["score"] for k in ("hybrid_tiles_4096", "wavefront", "bit_parallel")}) == 1
+    res["hybrid_equals_wavefront"] = bool(np.array_equal(braids["hybrid_tiles_4096"], braids["wavefront"]) and
+                                          np.array_equal(braids["hybrid_tiles_65536"], braids["wavefront"]))
+    res["scores_agree"] = len({res[k]["score"] for k in ("hybrid_tiles_4096", "hybrid_tiles_65536", "wavefront",
+                                                           "bit_parallel")}) == 1
     res["parity"] = check_pair_2p20(braids, res["bit_parallel"]["score"], m, n)
     # the reference's hybrid on a bounded sample: the leading 2^16 x 2^16 corner of the same pair
     sa, sb = a[:1 << 16].astype(np.int32), b[:1 << 16].astype(np.int32)

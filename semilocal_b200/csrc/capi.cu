@@ -131,6 +131,9 @@ int comb_wavefront_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int3
     return check_dev_err(err.p, s);
 }
 
+constexpr int kAutoTile = 1 << 16;         // tile edge of the hybrid the engine chooses by itself
+constexpr int kAutoHybridMin = 1 << 19;    // both lengths at least this: AUTO takes the hybrid
+
 // The last hybrid plan of each device, kept for the next call of the same shape (planning a hybrid -- tile
 // descriptors, glue levels, steady-ant plans, scratch -- costs far more host time than running a small one).  A
 // call that finds it busy or of another shape plans afresh and then offers its plan in its place.
@@ -145,8 +148,11 @@ HybridCache g_hcache[64];
 template <typename T>
 int comb_hybrid_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int32_t *d_r2c, int32_t *d_c2r,
                     int32_t *d_score, const slcs_opts *opts, cudaStream_t s) {
-    const int tr = (opts && opts->tile_rows > 0) ? opts->tile_rows : pick_tile();
-    const int tc = (opts && opts->tile_cols > 0) ? opts->tile_cols : pick_tile();
+    // tiles: the caller's, else for the engine's own choice of the hybrid (AUTO, large pairs) kAutoTile, else the
+    // tuned edge
+    const bool chosen = !opts || opts->algo == SLCS_ALGO_AUTO;
+    const int tr = (opts && opts->tile_rows > 0) ? opts->tile_rows : (chosen ? kAutoTile : pick_tile());
+    const int tc = (opts && opts->tile_cols > 0) ? opts->tile_cols : (chosen ? kAutoTile : pick_tile());
     HybridCache &C = g_hcache[E->device];
     HybridPlan *H = nullptr;
     bool from_cache = false;
@@ -199,14 +205,15 @@ int comb_hybrid_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int32_t
     return rc;
 }
 
-// Algorithm choice: the hybrid when asked for, or (AUTO) for grids large in both dimensions.
+// Algorithm choice: the hybrid when asked for, or (AUTO) for grids large in both dimensions, with tiles of
+// kAutoTile x kAutoTile: few enough glue levels (8 at 2^20) that the full occupancy of the tile combing outweighs
+// them.  Measured on B200, the 2^20 pair: hybrid with 65536-tiles 240 ms, wavefront 270-300 ms, hybrid with
+// 4096-tiles 370 ms (16 glue levels).
 bool use_hybrid(const slcs_opts *opts, int m, int n) {
     const int algo = opts ? opts->algo : SLCS_ALGO_AUTO;
     if (algo == SLCS_ALGO_HYBRID) return true;
     if (algo == SLCS_ALGO_WAVEFRONT) return false;
-    // AUTO: the wavefront.  It saturates the device once the pair has ~1000 bands, and on B200 it combed the 2^20
-    // pair in 357 ms against the hybrid's 461 ms (tiles 4096), whose glue tree is work the wavefront never does.
-    return false;
+    return std::min(m, n) >= kAutoHybridMin;
 }
 
 }  // namespace

@@ -67,13 +67,17 @@ def test_batch_4096_vs_reference(engine, digests, batch, mode, band_rows):
     _check_batch(res, sc, ref)
 
 
-@pytest.mark.parametrize("algo", ["wavefront", "hybrid"])
+@pytest.mark.parametrize("algo", ["wavefront", "hybrid", "hybrid_65536", "auto"])
 def test_pair_2p20_vs_reference(engine, digests, pair_2p20, algo):
     a, b = pair_2p20
     ref = digests["hybrid_2p20"]
     assert (len(a), len(b)) == (ref["m"], ref["n"])
     if algo == "hybrid":
         r2c, score = engine.comb(a, b, algo=engine.ALGO_HYBRID, tile=4096)
+    elif algo == "hybrid_65536":
+        r2c, score = engine.comb(a, b, algo=engine.ALGO_HYBRID, tile=65536)
+    elif algo == "auto":
+        r2c, score = engine.comb(a, b)
     else:
         r2c, score = engine.comb(a, b, algo=engine.ALGO_WAVEFRONT)
     assert _digest(r2c) == ref["sha256"]
