@@ -99,8 +99,7 @@ int comb_wavefront_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int3
     const int rows = swap ? n : m, cols = swap ? m : n;
 
     std::vector<CombItem> items;
-    const int cta_R = pick_rows_cta(rows, opts ? opts->band_rows : 0);
-    const int bands = cta_R ? plan_bands_uniform(rows, cta_R, items) : plan_bands(0, rows, swap ? Rb : Ra, items);
+    const int bands = plan_bands(0, rows, swap ? Rb : Ra, items);
     DevBuf<int32_t> c2r_tmp, prog, err;
     DevBuf<CombPair> dpair;
     DevBuf<CombItem> ditems;
@@ -122,10 +121,7 @@ int comb_wavefront_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int3
     SLCS_CUDA_TRY(cudaMemcpyAsync(dpair.p, &hp, sizeof(hp), cudaMemcpyHostToDevice, s));
     SLCS_CUDA_TRY(cudaMemcpyAsync(ditems.p, items.data(), sizeof(CombItem) * items.size(),
                                   cudaMemcpyHostToDevice, s));
-    if (cta_R)
-        SLCS_TRY(launch_comb_cta<T>(dpair.p, ditems.p, (int) items.size(), cta_R, next.p, err.p, E->num_sms, s));
-    else
-        SLCS_TRY(launch_comb_lone<T>(dpair.p, ditems.p, (int) items.size(), next.p, err.p, comb_resident_warps(E), s));
+    SLCS_TRY(launch_comb_lone<T>(dpair.p, ditems.p, (int) items.size(), next.p, err.p, comb_resident_warps(E), s));
     SLCS_TRY(launch_invert(c2r_work, size, d_r2c, swap, err.p, s));
     if (d_c2r != nullptr && swap) SLCS_TRY(launch_invert(d_r2c, size, d_c2r, false, err.p, s));
     return check_dev_err(err.p, s);

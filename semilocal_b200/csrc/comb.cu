@@ -14,8 +14,6 @@
 // symbols match or the left strand's id is larger than the top strand's.
 // Output (ends -> starts, R:include/SemiLocal/SemiLocalLCS.h:117-121): column j < n receives the strand
 // leaving the bottom of column j, column n+l the strand leaving the right side of row m-1-l.
-#include <algorithm>
-
 #include "slcs_internal.cuh"
 
 namespace slcs {
@@ -37,54 +35,9 @@ __device__ __forceinline__ void comb_cell(int A, int bs, int &L, int &t, int one
     t = nt;
 }
 
-// The shared-memory hand-off of the lone-pair kernel: the bands of one CTA pass their bottom strands to the next
-// band of the same CTA through a ring of kCtaRing 32-column chunks per band, with a produced / consumed chunk
-// counter per band (block-scope release / acquire), instead of through L2.
-constexpr int kCtaWarps = 8;   // bands (warps) per CTA
-constexpr int kCtaRing = 4;    // chunks per band's ring
-constexpr int kCtaMaxRows = 1 << 16;   // lone pairs up to this many rows take the CTA kernel
-struct CtaRing {
-    int data[kCtaWarps][kCtaRing][32];
-    int prod[kCtaWarps];   // output chunks band w has put in its ring
-    int cons[kCtaWarps];   // chunks of band w's ring the next band has taken
-};
-
-__device__ __forceinline__ int ld_acquire_block(const int *p) {
-    cuda::atomic_ref<int, cuda::thread_scope_block> r(*const_cast<int *>(p));
-    return r.load(cuda::memory_order_acquire);
-}
-__device__ __forceinline__ void st_release_block(int *p, int v) {
-    cuda::atomic_ref<int, cuda::thread_scope_block> r(*p);
-    r.store(v, cuda::memory_order_release);
-}
-// Waits (one lane) until the shared counter *p >= need, bounded like wait_at_least: gives up after the same time
-// limit (setting the error word) or when another thread reported an error.
-__device__ __forceinline__ bool wait_block_at_least(const int *p, int need, int *err) {
-    if (ld_acquire_block(p) >= need) return true;
-    const unsigned long long t0 = global_ns();
-    // a band waits for the band above it in the same CTA, which runs one chunk ahead: spin on the shared counter
-    // (no sleep, whose granularity would be added to every hand-off), checking the error word and the clock
-    // every 64 polls, and only after 2^14 polls sleep between polls
-    for (long long it = 0; it < (1ll << 28); ++it) {
-        if (it >= (1 << 14)) __nanosleep(32);
-        if (ld_acquire_block(p) >= need) return true;
-        if ((it & 63) == 63) {
-            if (ld_relaxed(err) != kDevErrNone) return false;
-            if (global_ns() - t0 > kWaitLimitNs) break;
-        }
-    }
-    raise_error(err, kDevErrTimeout);
-    return false;
-}
-
-// One band.  CTA = false: the band takes its top strands from the band above through the pair's c2r array and a
-// progress counter in global memory, and hands its bottom strands down the same way.  CTA = true (lone-pair
-// kernel): with in_s it takes them from the previous warp's ring in `rg`, with out_s it hands them to its own ring
-// (warp w's), otherwise through global memory as above.
-template <typename T, int R, int CH, bool CTA = false>
+template <typename T, int R, int CH>
 __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, int *err, int lane, int one,
-                                          int neg1, CtaRing *rg = nullptr, int w = 0, bool in_s = false,
-                                          bool out_s = false) {
+                                          int neg1) {
     static_assert(CH == 1 || (CH == 2 && R >= 2), "two chains need at least two rows per lane");
     const T *__restrict__ a = static_cast<const T *>(P.a);
     const T *__restrict__ b = static_cast<const T *>(P.b);
@@ -119,21 +72,6 @@ __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, 
         const int c0 = q << 5;
         io_b = pre_b;
         pre_b = c0 + 32 + lane < n ? static_cast<int>(b[c0 + 32 + lane]) : kSymColVirtual;
-        if (CTA && in_s) {
-            const int c = c0 + lane;
-            if (c0 < n) {
-                int ok = 1;
-                if (lane == 0) ok = wait_block_at_least(&rg->prod[w - 1], q + 1, err) ? 1 : 0;
-                ok = __shfl_sync(kFull, ok, 0);
-                if (!ok) return false;
-                io_t = c < n ? rg->data[w - 1][q % kCtaRing][lane] : kStrandPad;
-                __syncwarp();
-                if (lane == 0) st_release_block(&rg->cons[w - 1], q + 1);
-            } else {
-                io_t = kStrandPad;
-            }
-            return true;
-        }
         if (has_prev && c0 < n) {
             int ok = 1;
             if (lane == 0) ok = wait_at_least(prev_prog, min(n, c0 + 32), err) ? 1 : 0;
@@ -187,20 +125,6 @@ __device__ __forceinline__ void comb_band(const CombPair &P, const CombItem &I, 
         // io_t of lane j now holds the strand that left the band's bottom in column 32(q-CH)+j.
         const int col = ((q - CH) << 5) + lane;
         const bool valid = col >= 0 && col < n;
-        if (CTA && out_s) {
-            const int oc = q - CH;   // output chunk
-            if (oc >= 0 && (oc << 5) < n) {
-                int ok = 1;
-                if (lane == 0) ok = wait_block_at_least(&rg->cons[w], oc - kCtaRing + 1, err) ? 1 : 0;
-                ok = __shfl_sync(kFull, ok, 0);
-                if (!ok) return;
-                rg->data[w][oc % kCtaRing][lane] = io_t;
-                __syncwarp();
-                if (lane == 0) st_release_block(&rg->prod[w], oc + 1);
-            }
-            if (q + 1 < nchunks && !load(q + 1)) return;
-            continue;
-        }
         if (valid) __stcg(P.c2r + col, io_t);
         if (I.last && P.score != nullptr) {
             const unsigned bal = __ballot_sync(kFull, valid && io_t < m);
@@ -240,38 +164,6 @@ __global__ void __launch_bounds__(32, 12) comb_kernel(const CombPair *__restrict
             case 2: comb_band<T, 2, CH>(P, I, err, lane, one, neg1); break;
             default: comb_band<T, 1, 1>(P, I, err, lane, one, neg1); break;
         }
-    }
-}
-
-// Lone-pair kernel: CTAs of kCtaWarps warps take groups of kCtaWarps consecutive bands in order (a dequeue counter,
-// so a CTA only waits for bands of CTAs that dequeued before it); inside a CTA the bands hand their strands down
-// through shared memory, between CTAs through global memory.  All bands of the plan have R rows per lane.
-template <typename T, int R>
-__global__ void __launch_bounds__(32 * kCtaWarps) comb_cta_kernel(const CombPair *__restrict__ pairs,
-                                                              const CombItem *__restrict__ items, int nitems,
-                                                              int *next, int *err, int one, int neg1) {
-    __shared__ CtaRing rg;
-    __shared__ int group;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int ngroups = (nitems + kCtaWarps - 1) / kCtaWarps;
-    for (;;) {
-        if (threadIdx.x == 0) group = ld_relaxed(err) == kDevErrNone ? atomicAdd(next, 1) : ngroups;
-        if (threadIdx.x < kCtaWarps) {
-            rg.prod[threadIdx.x] = 0;
-            rg.cons[threadIdx.x] = 0;
-        }
-        __syncthreads();
-        const int g = group;
-        if (g >= ngroups) return;
-        const int it = g * kCtaWarps + w;
-        if (it < nitems) {
-            const CombItem I = items[it];
-            const CombPair P = pairs[I.pair];
-            const bool in_s = w > 0;
-            const bool out_s = w + 1 < kCtaWarps && it + 1 < nitems && !I.last;
-            comb_band<T, R, 1, true>(P, I, err, lane, one, neg1, &rg, w, in_s, out_s);
-        }
-        __syncthreads();   // the ring is reset for the next group only when every band of this one is done
     }
 }
 
@@ -343,41 +235,6 @@ int launch_comb_lone(const CombPair *d_pairs, const CombItem *d_items, int nitem
 }
 template int launch_comb_lone<uint8_t>(const CombPair *, const CombItem *, int, int *, int *, int, cudaStream_t);
 template int launch_comb_lone<int32_t>(const CombPair *, const CombItem *, int, int *, int *, int, cudaStream_t);
-
-template <typename T>
-int launch_comb_cta(const CombPair *d_pair, const CombItem *d_items, int nitems, int R, int *d_next, int *d_err,
-                    int num_sms, cudaStream_t s) {
-    if (nitems <= 0) return SLCS_OK;
-    const int groups = (nitems + kCtaWarps - 1) / kCtaWarps;
-    const int grid = std::min(groups, num_sms);
-    switch (R) {
-        case 1: comb_cta_kernel<T, 1><<<grid, 32 * kCtaWarps, 0, s>>>(d_pair, d_items, nitems, d_next, d_err, 1, -1); break;
-        case 2: comb_cta_kernel<T, 2><<<grid, 32 * kCtaWarps, 0, s>>>(d_pair, d_items, nitems, d_next, d_err, 1, -1); break;
-        case 4: comb_cta_kernel<T, 4><<<grid, 32 * kCtaWarps, 0, s>>>(d_pair, d_items, nitems, d_next, d_err, 1, -1); break;
-        case 8: comb_cta_kernel<T, 8><<<grid, 32 * kCtaWarps, 0, s>>>(d_pair, d_items, nitems, d_next, d_err, 1, -1); break;
-        default: return fail(SLCS_ERR_INTERNAL, "lone-pair CTA kernel: rows per lane must be 1, 2, 4 or 8");
-    }
-    SLCS_CUDA_TRY(cudaGetLastError());
-    return SLCS_OK;
-}
-template int launch_comb_cta<uint8_t>(const CombPair *, const CombItem *, int, int, int *, int *, int, cudaStream_t);
-template int launch_comb_cta<int32_t>(const CombPair *, const CombItem *, int, int, int *, int *, int, cudaStream_t);
-
-int pick_rows_cta(int rows, int band_rows) {
-    if (rows > kCtaMaxRows) return 0;
-    if (band_rows > 0) {   // the caller's band height, when the CTA kernel has it
-        const int R = band_rows / 32;
-        return (R == 1 || R == 2 || R == 4 || R == 8) && R * 32 == band_rows ? R : 0;
-    }
-    return rows <= 16384 ? 1 : 2;
-}
-
-int plan_bands_uniform(int m, int R, std::vector<CombItem> &items) {
-    const int rows = 32 * R;
-    const int bands = (m + rows - 1) / rows;
-    for (int b = 0; b < bands; ++b) items.push_back(CombItem{0, b, b * rows, R, b == bands - 1 ? 1 : 0});
-    return bands;
-}
 
 int comb_resident_warps_sm(int num_sms) {
     int per_sm = 0;

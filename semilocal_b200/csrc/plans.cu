@@ -20,8 +20,6 @@ struct slcs_pair_plan {
     int32_t *d_prog = nullptr, *d_c2r = nullptr;
     int *d_next = nullptr;
     int bands = 0, resident = 0;
-    int cta_R = 0;   // rows per lane of the CTA kernel, 0 = one-warp-per-band kernel
-    int num_sms = 0;
     const void *ba = nullptr, *bb = nullptr, *bscore = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // hybrid / bit
@@ -51,12 +49,8 @@ int wave_run(slcs_pair_plan *P, const uint8_t *d_a, const uint8_t *d_b, int32_t 
     if (d_score) SLCS_CUDA_TRY(cudaMemsetAsync(d_score, 0, sizeof(int32_t), s));
     const unsigned fl = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     SLCS_CUDA_TRY(cudaEventRecordWithFlags(P->ev0, s, fl));
-    if (P->cta_R)
-        SLCS_TRY(launch_comb_cta<uint8_t>(P->d_pair, P->d_items, (int) P->items.size(), P->cta_R, P->d_next,
-                                          P->d_err, P->num_sms, s));
-    else
-        SLCS_TRY(launch_comb_lone<uint8_t>(P->d_pair, P->d_items, (int) P->items.size(), P->d_next, P->d_err,
-                                           P->resident, s));
+    SLCS_TRY(launch_comb_lone<uint8_t>(P->d_pair, P->d_items, (int) P->items.size(), P->d_next, P->d_err,
+                                       P->resident, s));
     SLCS_CUDA_TRY(cudaEventRecordWithFlags(P->ev1, s, fl));
     SLCS_TRY(launch_invert(P->d_c2r, P->m + P->n, d_r2c, false, P->d_err, s));
     return SLCS_OK;
@@ -122,15 +116,9 @@ int slcs_pair_plan_create(int m, int n, int kind, const slcs_opts *opts, slcs_pa
     if ((rc = dalloc(reinterpret_cast<void **>(&P->d_err), sizeof(int), s))) return bail(rc);
     if (cudaMemsetAsync(P->d_err, 0, sizeof(int), s) != cudaSuccess) return bail(fail(SLCS_ERR_CUDA, "memset"));
     if (kind == SLCS_ALGO_WAVEFRONT) {
-        P->cta_R = pick_rows_cta(m, opts ? opts->band_rows : 0);
-        if (P->cta_R) {
-            P->bands = plan_bands_uniform(m, P->cta_R, P->items);
-        } else {
-            const int R = (opts && opts->band_rows > 0) ? std::max(1, opts->band_rows / 32) : pick_rows_single(m);
-            P->bands = plan_bands(0, m, R, P->items);
-        }
+        const int R = (opts && opts->band_rows > 0) ? std::max(1, opts->band_rows / 32) : pick_rows_single(m);
+        P->bands = plan_bands(0, m, R, P->items);
         P->resident = comb_resident_warps(E);
-        P->num_sms = E->num_sms;
         if ((rc = dalloc(reinterpret_cast<void **>(&P->d_items), sizeof(CombItem) * P->items.size(), s)) ||
             (rc = dalloc(reinterpret_cast<void **>(&P->d_pair), sizeof(CombPair), s)) ||
             (rc = dalloc(reinterpret_cast<void **>(&P->d_prog), sizeof(int32_t) * P->bands, s)) ||

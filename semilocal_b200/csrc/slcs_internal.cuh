@@ -181,16 +181,6 @@ int plan_bands(int pair, int m, int R, std::vector<CombItem> &items);
 template <typename T>
 int launch_comb(const CombPair *d_pairs, const CombItem *d_items, int nitems, int *d_next, int *d_err,
                 int grid_warps, cudaStream_t s);
-// The bands (all R rows per lane, planned by plan_bands_uniform) of one small pair alone on the device: CTAs of
-// consecutive bands that hand strands to each other through shared memory (comb.cu).  R in {1, 2, 4, 8}.
-template <typename T>
-int launch_comb_cta(const CombPair *d_pair, const CombItem *d_items, int nitems, int R, int *d_next, int *d_err,
-                    int num_sms, cudaStream_t s);
-int plan_bands_uniform(int m, int R, std::vector<CombItem> &items);
-// Rows per lane of the CTA kernel for a lone pair of `rows` rows (band_rows: the caller's band height, 0 = none);
-// 0 when the pair takes the one-warp-per-band kernel instead (more than 2^16 rows, or a band height the CTA kernel
-// does not have).
-int pick_rows_cta(int rows, int band_rows);
 // The same for the bands of one pair alone on the device: two dependency chains per lane (comb.cu).
 template <typename T>
 int launch_comb_lone(const CombPair *d_pairs, const CombItem *d_items, int nitems, int *d_next, int *d_err,

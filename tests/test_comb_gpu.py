@@ -78,21 +78,3 @@ def test_batch_vs_single(engine, oracle):
         assert np.array_equal(res0[i], exp), i
         assert np.array_equal(res1[i], exp), i
         assert sc0[i] == sc1[i] == oracle.global_score(exp, len(a), len(b)), i
-
-
-@pytest.mark.parametrize("band_rows", [32, 64, 128, 256])
-def test_lone_pair_cta_kernel(engine, oracle, band_rows):
-    """Small lone pairs take the kernel whose CTAs pass strands between their bands through shared memory: band
-    counts that do not fill a CTA, exactly one CTA, and more CTAs than SMs (so CTAs dequeue band groups), each
-    against the oracle; the same pair through the one-warp-per-band kernel (1024-row bands) agrees."""
-    rng = np.random.default_rng(band_rows + 1)
-    # (40000, 41000) keeps a as the rows: 40000 / band_rows bands, more groups of 8 than SMs at 32-row bands
-    for m, n in [(7, 300), (33, 33), (32 * 8 * (band_rows // 32), 500), (40000, 41000), (65536, 700), (1200, 9000)]:
-        a, b = _rand(rng, m, 4), _rand(rng, n, 4)
-        r2c, score = engine.comb(a, b, algo=engine.ALGO_WAVEFRONT, band_rows=band_rows)
-        exp = oracle.comb_antidiag(a, b, 8)
-        assert np.array_equal(r2c, exp), (m, n)
-        assert score == oracle.global_score(exp, m, n), (m, n)
-    a, b = _rand(rng, 5000, 4), _rand(rng, 4000, 4)
-    assert np.array_equal(engine.comb(a, b, algo=engine.ALGO_WAVEFRONT, band_rows=band_rows)[0],
-                          engine.comb(a, b, algo=engine.ALGO_WAVEFRONT, band_rows=1024)[0])
