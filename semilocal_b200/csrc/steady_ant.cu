@@ -1120,9 +1120,10 @@ __device__ __forceinline__ int band_row_count(const int32_t *X, int i0, int i1, 
     });
 }
 
-// warp-wide: as ballot_search, but the first 32 candidates are tried alone and the rest 256 at a time: most
-// searches end within a few columns, while a long one (a band whose column range spans a large part of the node,
-// as in the glue of the braids of two similar strings, read from global memory) then costs an eighth of the rounds
+// warp-wide: as ballot_search, but in rounds that grow: the first 32 candidates alone, the next 128 together, then
+// 1024 per round.  Most searches end within a few columns, while a long one (a band whose column range spans a
+// large part of the node, as in the glue of the braids of two similar strings, read from global memory) then takes
+// one load latency per 1024 columns instead of per 32.
 template <typename Pred>
 __device__ __forceinline__ int ballot_search_grow(int from, int end, int need, int none, int lane, Pred pred) {
     if (need <= 0) return from;
@@ -1130,7 +1131,25 @@ __device__ __forceinline__ int ballot_search_grow(int from, int end, int need, i
     const unsigned m = __ballot_sync(kFull, g < end && pred(g));
     const int cnt = __popc(m);
     if (need <= cnt) return from + (int) __fns(m, 0, need) + 1;
-    return ballot_search<8>(from + 32, end, need - cnt, none, lane, pred);
+    need -= cnt;
+    const int mid = min(end, from + 32 + 128);
+    int t = 0;   // raising candidates in [from + 32, mid)
+    {
+        bool q[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int h = from + 32 + 32 * u + lane;
+            q[u] = h < mid && pred(h);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const unsigned mu = __ballot_sync(kFull, q[u]);
+            const int c = __popc(mu);
+            if (t + c >= need) return from + 32 + 32 * u + (int) __fns(mu, 0, need - t) + 1;
+            t += c;
+        }
+    }
+    return ballot_search<32>(mid, end, need - t, none, lane, pred);
 }
 
 // warp-wide: one past the need-th column g in [from, cend) whose point raises delta in row R; k + 1 if none
@@ -1202,7 +1221,7 @@ __device__ __forceinline__ void band_warp_walk(int32_t *X, const YView &Y, int k
 
 // One CTA per band of kBand rows of a node: c* at every kBandSub rows (scans from the band's bottom), then
 // at every kBandWalk rows (each warp bottom-up through its sub-band), then walks of kBandWalk rows.
-__global__ void __launch_bounds__(kBandThreads) sa_band_kernel(const SaNode *__restrict__ nodes,
+__global__ void __launch_bounds__(kBandThreads, 3) sa_band_kernel(const SaNode *__restrict__ nodes,
                                                                const int2 *__restrict__ tasks,
                                                                const int32_t *__restrict__ xs,
                                                                const int32_t *__restrict__ ys,
