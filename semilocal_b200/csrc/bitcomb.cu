@@ -16,8 +16,9 @@
 //   * match and update are 4 three-input logic ops.
 // About 8 instructions per 32 cells.  A lane's strips follow each other one 32-step block apart and update
 // independently; lanes are (strips per lane + 1) blocks apart and pass one word per block by shuffle; warps
-// (bands of 32 x RS strips) are chained through a hand-off word array and a progress counter per band,
-// exactly like the integer combing kernel.
+// (bands of 32 x RS strips) are chained through an array of hand-off words, each stored together with the tag of
+// the band that wrote it in one 64-bit word: the band below polls the words it needs until they carry the tag of
+// the band above, so no release fence or progress counter sits between them.
 #include <algorithm>
 #include <cstdlib>
 
@@ -30,8 +31,8 @@ struct BitPair {
     const uint32_t *a1, *a0;        // row planes, word w = rows [32 w, 32 w + 32), bit i = row 32 w + i
     const uint32_t *b1, *b0, *b2;   // column planes, index q + 2 = columns [32 q, 32 q + 32), MSB first;
                                     // b2 = 1 outside [0, n); indices 0, 1 are leading pad words
-    uint32_t *hand;                 // hand-off words between bands: word q = columns [32 q, 32 q + 32)
-    int32_t *progress;              // per band: number of hand-off words written
+    unsigned long long *hand;       // hand-off words between bands: word q = columns [32 q, 32 q + 32) in the low
+                                    // half, (index of the band that wrote it) + 1 in the high half
     int32_t *ones;                  // out: popcount of the final left strands over real rows
     int m, n, nstrips, nblocks;
 };
@@ -40,7 +41,34 @@ struct BitItem {
     int pair, band, s0, last;
 };
 
-constexpr int kChunk = 16;   // hand-off words between bands are published / polled in groups of kChunk
+constexpr int kChunk = 8;   // hand-off words a band requests together (one chunk ahead of their use)
+
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long *p) {
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*const_cast<unsigned long long *>(p));
+    return r.load(cuda::memory_order_relaxed);
+}
+__device__ __forceinline__ void st_relaxed64(unsigned long long *p, unsigned long long v) {
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*p);
+    r.store(v, cuda::memory_order_relaxed);
+}
+// Until the hand-off word *p (already read into v) carries `tag` in its high half: re-reads it, polling without
+// sleeping first, bounded like wait_at_least (the error word is set when it gives up).  Data and tag travel in one
+// 64-bit store, so a word with the right tag is the right word.
+__device__ __forceinline__ bool wait_tag(const unsigned long long *p, unsigned long long &v, unsigned tag, int *err) {
+    if ((unsigned) (v >> 32) == tag) return true;
+    const unsigned long long t0 = global_ns();
+    for (long long it = 0; it < (1ll << 26); ++it) {
+        if (it >= kSpinPolls) __nanosleep(kSpinSleepNs);
+        v = ld_relaxed64(p);
+        if ((unsigned) (v >> 32) == tag) return true;
+        if ((it & 15) == 15) {
+            if (ld_relaxed(err) != kDevErrNone) return false;
+            if (global_ns() - t0 > kWaitLimitNs) break;
+        }
+    }
+    raise_error(err, kDevErrTimeout);
+    return false;
+}
 
 // One band (warp).  Lane k owns strips s0 + k RS + r, r = 0..RS-1.  The strips of a lane form one systolic
 // chain: strip r works one 32-step block behind strip r-1 and takes its input bit, each step, straight from
@@ -70,6 +98,8 @@ __device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int
     const int gmax = 31 * (RS + 1) + RS - 1 + nb;
     uint32_t carry = 0u;    // input word of strip 0, from the lane above (previous iteration)
     uint32_t chunkw = 0u;   // lanes 0..kChunk-1: the current chunk of hand-off words from the band above
+    unsigned long long nextw = 0ull;   // lanes 0..kChunk-1: the next chunk, requested one chunk ahead
+    const unsigned tag_above = (unsigned) I.band;   // tag of the band above: its index + 1
     // Column-plane words (index 0 .. nb + 2) reach the lanes through a ring in shared memory: the warp loads
     // 32 words per plane every 32 iterations, 64 words ahead, and stores them one iteration later, so no load
     // latency sits on the loop.  At iteration g the lanes read words >= g - 31 (RS + 1) - RS + 1 and <= g + 3;
@@ -112,14 +142,17 @@ __device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int
                 s2 = __ldg(P.b2 + idx);
             }
         }
-        // lane 0's input word: from the band above (zero strands for the first band).  The band above is
-        // polled once per kChunk words; the chunk's words are then loaded by lanes 0..kChunk-1 in one go and
-        // handed to lane 0 by shuffle, one per iteration.
+        // lane 0's input word: from the band above (zero strands for the first band).  Lanes 0..kChunk-1 read one
+        // word each of the next chunk a chunk ahead; at the chunk's start each waits until its word carries the
+        // band above's tag, and the words reach lane 0 by shuffle, one per iteration.
         if (I.band > 0 && g < nb && (g % kChunk) == 0) {
-            int ok = 1;
-            if (lane == 0) ok = wait_at_least(P.progress + (I.band - 1), min(nb, g + kChunk), err) ? 1 : 0;
-            if (!__shfl_sync(kFull, ok, 0)) return;   // the bounded wait gave up (error word set)
-            chunkw = (lane < kChunk && g + lane < nb) ? __ldcg(P.hand + g + lane) : 0u;
+            const bool mine = lane < kChunk && g + lane < nb;
+            if (g == 0 && mine) nextw = ld_relaxed64(P.hand + lane);
+            unsigned long long v = nextw;
+            const bool ok = !mine || wait_tag(P.hand + g + lane, v, tag_above, err);
+            if (!__all_sync(kFull, ok)) return;   // a bounded wait gave up (error word set)
+            chunkw = (uint32_t) v;
+            nextw = (lane < kChunk && g + kChunk + lane < nb) ? ld_relaxed64(P.hand + g + kChunk + lane) : 0ull;
         }
         const uint32_t hw = __shfl_sync(kFull, chunkw, g % kChunk);
         uint32_t io = lane == 0 ? ((I.band > 0 && g < nb) ? hw : 0u) : carry;
@@ -162,14 +195,10 @@ __device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int
         }
         // `out` holds the last strip's bottom-row outputs of its block g - lag - (RS - 1) minus one
         const int w = g - lag - RS;
-        if (lane == 31 && !I.last && w >= 0 && w < nb) {
-            __stcg(P.hand + w, out);
-            // publish once per kChunk words; the release store orders this lane's earlier stores before it
-            if ((w + 1) % kChunk == 0 || w + 1 == nb) st_release(P.progress + I.band, w + 1);
-        }
+        if (lane == 31 && !I.last && w >= 0 && w < nb)
+            st_relaxed64(P.hand + w, ((unsigned long long) (I.band + 1) << 32) | out);
         carry = __shfl_up_sync(kFull, out, 1);
     }
-    if (!I.last && lane == 31) st_release(P.progress + I.band, nb);
     int ones = 0;
 #pragma unroll
     for (int r = 0; r < RS; ++r)
@@ -250,8 +279,9 @@ __global__ void bit_score_kernel(const int32_t *ones, int m, int32_t *score) {
 
 struct BitPlan {
     int m = 0, n = 0, nstrips = 0, nblocks = 0, nbw = 0, RS = 1, bands = 0, warps = 0;
-    uint32_t *a1 = nullptr, *a0 = nullptr, *b1 = nullptr, *b0 = nullptr, *b2 = nullptr, *hand = nullptr;
-    int32_t *prog = nullptr, *ones = nullptr;
+    uint32_t *a1 = nullptr, *a0 = nullptr, *b1 = nullptr, *b0 = nullptr, *b2 = nullptr;
+    unsigned long long *hand = nullptr;
+    int32_t *ones = nullptr;
     int *next = nullptr;
     BitPair *dp = nullptr;
     BitItem *di = nullptr;
@@ -261,7 +291,7 @@ struct BitPlan {
 
 void bit_plan_destroy(BitPlan *B) {
     if (!B) return;
-    void *ps[] = {B->a1, B->a0, B->b1, B->b0, B->b2, B->hand, B->prog, B->ones, B->next, B->dp, B->di};
+    void *ps[] = {B->a1, B->a0, B->b1, B->b0, B->b2, B->hand, B->ones, B->next, B->dp, B->di};
     for (void *p : ps) dfree(p, B->s);
     if (B->ev0) cudaEventDestroy(B->ev0);
     if (B->ev1) cudaEventDestroy(B->ev1);
@@ -293,13 +323,12 @@ int bit_plan_create(Engine *E, int m, int n, cudaStream_t s, BitPlan **out) {
     BP_ALLOC(b0, B->nbw);
     BP_ALLOC(b2, B->nbw);
     BP_ALLOC(hand, B->nblocks + 1);
-    BP_ALLOC(prog, B->bands);
     BP_ALLOC(ones, 1);
     BP_ALLOC(next, 1);
     BP_ALLOC(dp, 1);
     BP_ALLOC(di, B->bands);
 #undef BP_ALLOC
-    BitPair hp{B->a1, B->a0, B->b1, B->b0, B->b2, B->hand, B->prog, B->ones, m, n, B->nstrips, B->nblocks};
+    BitPair hp{B->a1, B->a0, B->b1, B->b0, B->b2, B->hand, B->ones, m, n, B->nstrips, B->nblocks};
     std::vector<BitItem> items(B->bands);
     for (int b = 0; b < B->bands; ++b) items[b] = BitItem{0, b, b * per_band, b == B->bands - 1 ? 1 : 0};
     if (cudaMemcpyAsync(B->dp, &hp, sizeof(hp), cudaMemcpyHostToDevice, s) != cudaSuccess ||
@@ -324,10 +353,9 @@ int bit_plan_run(BitPlan *B, const uint8_t *d_a, const uint8_t *d_b, int32_t *d_
         SLCS_CUDA_TRY(cudaMemsetAsync(d_score, 0, sizeof(int32_t), s));
         return SLCS_OK;
     }
-    SLCS_CUDA_TRY(cudaMemsetAsync(B->prog, 0, sizeof(int32_t) * B->bands, s));
     SLCS_CUDA_TRY(cudaMemsetAsync(B->ones, 0, sizeof(int32_t), s));
     SLCS_CUDA_TRY(cudaMemsetAsync(B->next, 0, sizeof(int), s));
-    SLCS_CUDA_TRY(cudaMemsetAsync(B->hand, 0, sizeof(uint32_t) * (B->nblocks + 1), s));
+    SLCS_CUDA_TRY(cudaMemsetAsync(B->hand, 0, sizeof(unsigned long long) * (B->nblocks + 1), s));
     const int pack_warps = B->nstrips + B->nbw;
     bit_pack_kernel<<<std::min(4096, (pack_warps + 7) / 8), 256, 0, s>>>(d_a, B->m, d_b, B->n, B->nstrips, B->nbw, B->a1,
                                                                          B->a0, B->b1, B->b0, B->b2, d_err);
