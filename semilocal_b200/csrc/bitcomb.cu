@@ -145,14 +145,16 @@ __device__ __forceinline__ void bit_band(const BitPair &P, const BitItem &I, int
         // lane 0's input word: from the band above (zero strands for the first band).  Lanes 0..kChunk-1 read one
         // word each of the next chunk a chunk ahead; at the chunk's start each waits until its word carries the
         // band above's tag, and the words reach lane 0 by shuffle, one per iteration.
+        // The band above writes words 0 .. nb - 2 (block nb - 1 lies wholly past the string's end and leaves its
+        // last strip after the band's final iteration): the last word is taken as zero strands, unwaited.
         if (I.band > 0 && g < nb && (g % kChunk) == 0) {
-            const bool mine = lane < kChunk && g + lane < nb;
+            const bool mine = lane < kChunk && g + lane < nb - 1;
             if (g == 0 && mine) nextw = ld_relaxed64(P.hand + lane);
             unsigned long long v = nextw;
             const bool ok = !mine || wait_tag(P.hand + g + lane, v, tag_above, err);
             if (!__all_sync(kFull, ok)) return;   // a bounded wait gave up (error word set)
-            chunkw = (uint32_t) v;
-            nextw = (lane < kChunk && g + kChunk + lane < nb) ? ld_relaxed64(P.hand + g + kChunk + lane) : 0ull;
+            chunkw = mine ? (uint32_t) v : 0u;
+            nextw = (lane < kChunk && g + kChunk + lane < nb - 1) ? ld_relaxed64(P.hand + g + kChunk + lane) : 0ull;
         }
         const uint32_t hw = __shfl_sync(kFull, chunkw, g % kChunk);
         uint32_t io = lane == 0 ? ((I.band > 0 && g < nb) ? hw : 0u) : carry;
