@@ -1152,12 +1152,38 @@ __device__ __forceinline__ int ballot_search_grow(int from, int end, int need, i
     return ballot_search<32>(mid, end, need - t, none, lane, pred);
 }
 
+// warp-wide, columns in global memory (a band whose column range was too wide to stage): one past the need-th
+// column g in [from, end) whose point raises delta in row R, `none` if there are fewer.  Rounds of 512 columns, each
+// lane loading its 16 columns unconditionally (indices clamped into the range) before testing any, so that a round
+// costs one load latency: a search across the step of a nearly step-shaped demarcation line spans most of the node.
+__device__ __forceinline__ int global_col_search(const int32_t *__restrict__ ycol, int from, int end, int need, int R,
+                                                 int none, int lane) {
+    constexpr int U = 16;
+    for (int g0 = from; g0 < end; g0 += 32 * U) {
+        int v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) v[u] = __ldg(ycol + min(g0 + 32 * u + lane, end - 1));
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int y = v[u] & kValMask;
+            const bool q = g0 + 32 * u + lane < end && ((v[u] & kHiBit) ? (y < R) : (y >= R));
+            const unsigned m = __ballot_sync(kFull, q);
+            const int cnt = __popc(m);
+            if (need <= cnt) return g0 + 32 * u + (int) __fns(m, 0, need) + 1;
+            need -= cnt;
+        }
+    }
+    return none;
+}
+
 // warp-wide: one past the need-th column g in [from, cend) whose point raises delta in row R; k + 1 if none
-// (U = 0: the growing search above)
+// (U = 0: the growing search above on staged columns; columns left in global memory always take the batched one)
 template <int U = 0>
 __device__ __forceinline__ int band_col_search(const YView &Y, int k, int from, int cend, int need, int R, int lane) {
+    if (need <= 0) return from;
+    if (!Y.in_smem) return global_col_search(Y.g, from, cend, need, R, k + 1, lane);
     auto pred = [&](int g) {
-        const int w = Y(g);
+        const int w = Y.s[g - Y.clo];
         const int y = w & kValMask;
         return (w & kHiBit) ? (y < R) : (y >= R);
     };
@@ -1292,7 +1318,9 @@ __global__ void __launch_bounds__(kBandThreads, 3) sa_band_kernel(const SaNode *
     if (tid < nwalk) {
         const int i0 = tid * kBandWalk, i1 = min(i0 + kBandWalk, nr);
         const int c0 = S.cst[tid + 1], ce = S.cst[tid];
-        if (min(ce, k) - min(c0, k) <= kWalkSpanMax) band_thread_walk(S.x, Y, k, R0, i0, i1, c0, cend);
+        // (with the columns in global memory every walk goes to a warp: a thread's column scan would be a chain of
+        // dependent loads)
+        if (ysm && min(ce, k) - min(c0, k) <= kWalkSpanMax) band_thread_walk(S.x, Y, k, R0, i0, i1, c0, cend);
         else S.queue[atomicAdd(&S.nq, 1)] = tid;
     }
     __syncthreads();
