@@ -58,7 +58,10 @@ typedef struct slcs_opts {
     int tile_cols;       /* hybrid tile width  (0 = default 4096) */
     int band_rows;       /* wavefront rows per warp band: 32*R, R in {1,2,4,8,16,32} (0 = auto) */
     int sa_cutoff;       /* steady-ant size below which sub-problems finish in shared memory (0 = default) */
-    int reserved[3];
+    int lane_cols;       /* wavefront of a lone pair: columns a lane combs per step -- 4 or 8 = register tiles of
+                            band_rows/32 x lane_cols cells (band_rows 64..512, else 256), 1 = one column per step
+                            (the band kernel), 0 = auto: tiles of 8 x 4 up to 131072 rows unless band_rows is given */
+    int reserved[2];
 } slcs_opts;
 
 /* ---- library ------------------------------------------------------------------------------------ */

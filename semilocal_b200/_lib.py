@@ -31,7 +31,8 @@ class SlcsError(RuntimeError):
 
 class Opts(ctypes.Structure):
     _fields_ = [("algo", ctypes.c_int), ("tile_rows", ctypes.c_int), ("tile_cols", ctypes.c_int),
-                ("band_rows", ctypes.c_int), ("sa_cutoff", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
+                ("band_rows", ctypes.c_int), ("sa_cutoff", ctypes.c_int), ("lane_cols", ctypes.c_int),
+                ("reserved", ctypes.c_int * 2)]
 
 
 class Query(ctypes.Structure):
@@ -191,7 +192,9 @@ def check(rc: int) -> None:
         raise SlcsError(rc, msg.decode(errors="replace") if msg else "")
 
 
-def opts(algo: int = ALGO_AUTO, tile_rows: int = 0, tile_cols: int = 0, band_rows: int = 0, sa_cutoff: int = 0):
+def opts(algo: int = ALGO_AUTO, tile_rows: int = 0, tile_cols: int = 0, band_rows: int = 0, sa_cutoff: int = 0,
+         lane_cols: int = 0):
     o = Opts()
     o.algo, o.tile_rows, o.tile_cols, o.band_rows, o.sa_cutoff = algo, tile_rows, tile_cols, band_rows, sa_cutoff
+    o.lane_cols = lane_cols
     return o

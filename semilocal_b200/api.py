@@ -65,15 +65,16 @@ class Permutation:
 
 
 def comb(a, b, algo: int = _lib.ALGO_AUTO, tile: int = 0, band_rows: int = 0, want_col_to_row: bool = False,
-         sa_cutoff: int = 0) -> Tuple[np.ndarray, int]:
-    """Braid (row->col, m+n int32) and global LLCS of the pair (a, b)."""
+         sa_cutoff: int = 0, lane_cols: int = 0) -> Tuple[np.ndarray, int]:
+    """Braid (row->col, m+n int32) and global LLCS of the pair (a, b).  lane_cols picks the wavefront kernel of a
+    lone pair (4: register tiles, 1: one column per lane step, 0: automatic)."""
     a_arr = np.ascontiguousarray(np.asarray(a))
     b_arr = np.ascontiguousarray(np.asarray(b))
     m, n = len(a_arr), len(b_arr)
     r2c = np.empty(m + n, dtype=np.int32)
     c2r = np.empty(m + n, dtype=np.int32) if want_col_to_row else None
     score = ctypes.c_int32(0)
-    o = _lib.opts(algo, tile, tile, band_rows, sa_cutoff)
+    o = _lib.opts(algo, tile, tile, band_rows, sa_cutoff, lane_cols)
     wide = a_arr.dtype != np.uint8 or b_arr.dtype != np.uint8
     if wide and ((a_arr.size and (a_arr.min() < 0 or a_arr.max() > 255)) or
                  (b_arr.size and (b_arr.min() < 0 or b_arr.max() > 255))):
@@ -283,8 +284,8 @@ class PairPlan:
     """A reusable single-pair plan on device buffers (include/slcs.h: slcs_pair_plan_*): kind is ALGO_WAVEFRONT,
     ALGO_HYBRID or PLAN_BITPARALLEL.  run() takes device pointers (ints) and a stream handle."""
 
-    def __init__(self, m: int, n: int, kind: int, tile: int = 0, band_rows: int = 0):
-        o = _lib.opts(kind if kind != _lib.PLAN_BITPARALLEL else 0, tile, tile, band_rows)
+    def __init__(self, m: int, n: int, kind: int, tile: int = 0, band_rows: int = 0, lane_cols: int = 0):
+        o = _lib.opts(kind if kind != _lib.PLAN_BITPARALLEL else 0, tile, tile, band_rows, 0, lane_cols)
         h = ctypes.c_void_p()
         check(lib().slcs_pair_plan_create(m, n, kind, ctypes.byref(o), ctypes.byref(h)))
         self.h, self.m, self.n, self.kind = h, m, n, kind

@@ -43,33 +43,6 @@ struct BitItem {
 
 constexpr int kChunk = 8;   // hand-off words a band requests together (one chunk ahead of their use)
 
-__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long *p) {
-    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*const_cast<unsigned long long *>(p));
-    return r.load(cuda::memory_order_relaxed);
-}
-__device__ __forceinline__ void st_relaxed64(unsigned long long *p, unsigned long long v) {
-    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*p);
-    r.store(v, cuda::memory_order_relaxed);
-}
-// Until the hand-off word *p (already read into v) carries `tag` in its high half: re-reads it, polling without
-// sleeping first, bounded like wait_at_least (the error word is set when it gives up).  Data and tag travel in one
-// 64-bit store, so a word with the right tag is the right word.
-__device__ __forceinline__ bool wait_tag(const unsigned long long *p, unsigned long long &v, unsigned tag, int *err) {
-    if ((unsigned) (v >> 32) == tag) return true;
-    const unsigned long long t0 = global_ns();
-    for (long long it = 0; it < (1ll << 26); ++it) {
-        if (it >= kSpinPolls) __nanosleep(kSpinSleepNs);
-        v = ld_relaxed64(p);
-        if ((unsigned) (v >> 32) == tag) return true;
-        if ((it & 15) == 15) {
-            if (ld_relaxed(err) != kDevErrNone) return false;
-            if (global_ns() - t0 > kWaitLimitNs) break;
-        }
-    }
-    raise_error(err, kDevErrTimeout);
-    return false;
-}
-
 // One band (warp).  Lane k owns strips s0 + k RS + r, r = 0..RS-1.  The strips of a lane form one systolic
 // chain: strip r works one 32-step block behind strip r-1 and takes its input bit, each step, straight from
 // strip r-1's bottom row (so the RS strips of a lane update independently every step); lanes are RS+1 blocks

@@ -99,7 +99,10 @@ int comb_wavefront_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int3
     const int rows = swap ? n : m, cols = swap ? m : n;
 
     std::vector<CombItem> items;
-    const int bands = plan_bands(0, rows, swap ? Rb : Ra, items);
+    const TileShape ts = tile_shape_for(rows, opts ? opts->band_rows : 0, opts ? opts->lane_cols : 0);
+    const int Rt = ts.R;
+    const int bands = Rt > 0 ? plan_tile_bands(0, rows, Rt, items) : plan_bands(0, rows, swap ? Rb : Ra, items);
+    DevBuf<unsigned long long> hand;
     DevBuf<int32_t> c2r_tmp, prog, err;
     DevBuf<CombPair> dpair;
     DevBuf<CombItem> ditems;
@@ -110,18 +113,26 @@ int comb_wavefront_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int3
         c2r_work = c2r_tmp.p;
     }
     SLCS_TRY(prog.alloc(bands, s));
+    if (Rt > 0) {
+        SLCS_TRY(hand.alloc(cols, s));
+        SLCS_CUDA_TRY(cudaMemsetAsync(hand.p, 0, sizeof(unsigned long long) * cols, s));
+    }
     SLCS_TRY(err.alloc(1, s));
     SLCS_TRY(dpair.alloc(1, s));
     SLCS_TRY(ditems.alloc(items.size(), s));
     SLCS_TRY(next.alloc(1, s));
-    CombPair hp{rows_s, cols_s, c2r_work, prog.p, d_score, rows, cols};
+    CombPair hp{rows_s, cols_s, c2r_work, prog.p, d_score, rows, cols, hand.p};
     SLCS_CUDA_TRY(cudaMemsetAsync(prog.p, 0, sizeof(int32_t) * bands, s));
     SLCS_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(int), s));
     SLCS_CUDA_TRY(cudaMemsetAsync(next.p, 0, sizeof(int), s));
     SLCS_CUDA_TRY(cudaMemcpyAsync(dpair.p, &hp, sizeof(hp), cudaMemcpyHostToDevice, s));
     SLCS_CUDA_TRY(cudaMemcpyAsync(ditems.p, items.data(), sizeof(CombItem) * items.size(),
                                   cudaMemcpyHostToDevice, s));
-    SLCS_TRY(launch_comb_lone<T>(dpair.p, ditems.p, (int) items.size(), next.p, err.p, comb_resident_warps(E), s));
+    if (Rt > 0)
+        SLCS_TRY(launch_comb_tile<T>(dpair.p, ditems.p, (int) items.size(), next.p, err.p, comb_resident_warps(E),
+                                     ts.C, s));
+    else
+        SLCS_TRY(launch_comb_lone<T>(dpair.p, ditems.p, (int) items.size(), next.p, err.p, comb_resident_warps(E), s));
     SLCS_TRY(launch_invert(c2r_work, size, d_r2c, swap, err.p, s));
     if (d_c2r != nullptr && swap) SLCS_TRY(launch_invert(d_r2c, size, d_c2r, false, err.p, s));
     return check_dev_err(err.p, s);

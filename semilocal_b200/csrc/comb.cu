@@ -167,6 +167,187 @@ __global__ void __launch_bounds__(32, 12) comb_kernel(const CombPair *__restrict
     }
 }
 
+// ---- lone pairs: register tiles ----
+//
+// A pair alone on the device gets few bands, one warp each, and a warp alone on its SM sub-partition is bound by
+// its own latency, not by issue: each step of the band kernel above waits for the shuffle bringing the strand from
+// the lane above, so a step costs a shuffle's latency however few rows the lane combs.  Here a lane combs a tile
+// of R rows x C columns per step: the C strands arriving from the lane above travel in C independent shuffles
+// (one latency per step), and the R x C cells form a small wavefront with C-fold parallelism.  Everything
+// else works per sub-chunk of 32 columns (K = 32 / C steps):
+//   * b-symbols go through a ring of 256 (C = 4) or 512 (C = 8) columns in shared memory (as ints, padding columns
+//     kSymColVirtual), one column per lane per sub-chunk, loaded one sub-chunk ahead; each step reads its C
+//     symbols in 16-byte accesses;
+//   * lane 0's input strands of sub-chunk j come from the band above through the pair's hand-off words, each
+//     carrying the writing band's tag (band + 1) beside the strand in one 64-bit word: loaded one sub-chunk ahead
+//     and polled (bounded) only while the tag is not there yet;
+//   * lane 31's bottom strands are staged in shared memory and published 32 words at a time (coalesced) as soon
+//     as a sub-chunk is complete, two steps after its last group left the warp.  The last band writes them to c2r
+//     instead (they are final) and counts the score.
+// The band kernel's persistent in-order dequeue is kept: a band only waits for a band a running warp owns.
+// Measured on B200 (8192 x 8192, one warp per band): a step of an 8 x 4 tile takes ~330 cycles against ~240 for
+// 4 x 4 and ~76 for the band kernel's one column of four rows, and a band starts ~47 steps after the one above
+// (32 for the lanes, the rest the hand-off); the whole pair takes 0.61 ms against 0.86-1.0 ms.
+// C consecutive ints of shared memory in 16-byte accesses (C a multiple of 4, the address 16-byte aligned)
+template <int C>
+__device__ __forceinline__ void lds_ints(const int *p, int (&o)[C]) {
+#pragma unroll
+    for (int i = 0; i < C; i += 4) {
+        const int4 v = *reinterpret_cast<const int4 *>(p + i);
+        o[i] = v.x;
+        o[i + 1] = v.y;
+        o[i + 2] = v.z;
+        o[i + 3] = v.w;
+    }
+}
+template <int C>
+__device__ __forceinline__ void sts_ints(int *p, const int (&v)[C]) {
+#pragma unroll
+    for (int i = 0; i < C; i += 4) *reinterpret_cast<int4 *>(p + i) = make_int4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+}
+
+// symbol ring: the columns a step can read span 31 C + 32 behind the newest sub-chunk, plus the sub-chunk
+// written ahead; a power of two above that
+template <int C>
+struct TileShared {
+    static constexpr int kRing = C <= 4 ? 256 : 512;
+    int sym[kRing];   // b-symbols of columns c (at c & (kRing - 1)) as ints
+    int tin[64];      // lane 0's input strands of two sub-chunks (column c at c & 63)
+    int tout[64];     // lane 31's output strands of two sub-chunks (column c at c & 63)
+};
+
+template <typename T, int R, int C>
+__device__ __forceinline__ void comb_tile_band(const CombPair &P, const CombItem &I, int *err, int lane, int one,
+                                               int neg1, TileShared<C> &S) {
+    static_assert(C == 4 || C == 8, "tile widths 4 and 8");
+    constexpr int K = 32 / C;   // steps per sub-chunk of 32 columns
+    constexpr int SB = TileShared<C>::kRing;
+    const T *__restrict__ a = static_cast<const T *>(P.a);
+    const T *__restrict__ b = static_cast<const T *>(P.b);
+    const int m = P.m, n = P.n;
+    const int rbase = I.r0 + lane * R;
+
+    int A[R], L[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int row = rbase + k;
+        if (row < m) {
+            A[k] = static_cast<int>(a[row]);
+            L[k] = m - 1 - row;
+        } else {
+            A[k] = kSymRowVirtual;
+            L[k] = -1;
+        }
+    }
+    const int G = (n + C - 1) / C;               // column groups; lane l combs group s - l at step s
+    const int nsub = (G + 31 + K - 1) / K;       // sub-chunks of steps
+    const int Q = (n + 31) >> 5;                 // sub-chunks of columns
+    const bool has_prev = I.band > 0;
+    const unsigned tag_above = (unsigned) I.band;                                  // the band above: its index + 1
+    const unsigned long long my_tag = (unsigned long long) (I.band + 1) << 32;
+
+    __syncwarp();   // the previous band's last reads of S are done
+    for (int i = lane; i < SB; i += 32) S.sym[i] = kSymColVirtual;
+    int pb = lane < n ? static_cast<int>(b[lane]) : kSymColVirtual;
+    unsigned long long pw = (has_prev && lane < n) ? ld_relaxed64(P.hand + lane) : 0ull;
+
+    int t[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) t[c] = kStrandPad;
+    int cnt = 0;   // last band: bottom strands < m (the score)
+    int qpub = 0;  // next sub-chunk of columns to publish
+
+    // publishes every column sub-chunk whose groups all left the warp before step `done` (exclusive)
+    auto publish = [&](int done) {
+        while (qpub < Q && min((qpub + 1) * K, G) + 31 <= done) {
+            const int col = (qpub << 5) + lane;
+            if (col < n) {
+                const int v = S.tout[col & 63];
+                if (I.last) {
+                    P.c2r[col] = v;
+                    cnt += v < m;
+                } else {
+                    st_relaxed64(P.hand + col, my_tag | (unsigned) v);
+                }
+            }
+            ++qpub;
+        }
+    };
+
+    for (int j = 0; j < nsub; ++j) {
+        const int col = (j << 5) + lane;
+        int in = kStrandPad;
+        bool ok = true;
+        if (col < n) {
+            if (!has_prev) in = m + col;
+            else {
+                ok = wait_tag(P.hand + col, pw, tag_above, err);
+                in = (int) (unsigned) pw;
+            }
+        }
+        if (!__all_sync(kFull, ok)) return;
+        publish(j * K);   // reads S.tout written before the last __syncwarp
+        S.tin[col & 63] = in;
+        S.sym[col & (SB - 1)] = pb;
+        const int ncol = col + 32;
+        pb = ncol < n ? static_cast<int>(b[ncol]) : kSymColVirtual;
+        if (has_prev && ncol < n) pw = ld_relaxed64(P.hand + ncol);
+        __syncwarp();
+        const int tin_base = (j & 1) << 5;
+        const int sym_base = (j * K - lane) * C;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            int x[C], bs[C];
+            lds_ints<C>(S.tin + tin_base + k * C, x);
+            lds_ints<C>(S.sym + ((sym_base + k * C) & (SB - 1)), bs);
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const int u = __shfl_up_sync(kFull, t[c], 1);
+                t[c] = lane == 0 ? x[c] : u;
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int c = 0; c < C; ++c) comb_cell(A[r], bs[c], L[r], t[c], one, neg1);
+            const int g = j * K + k - 31;
+            if (lane == 31 && g >= 0 && g < G) sts_ints<C>(S.tout + ((g * C) & 63), t);
+        }
+        __syncwarp();
+    }
+    publish(nsub * K);
+    if (I.last && P.score != nullptr) {
+        const int tot = __reduce_add_sync(kFull, cnt);
+        if (lane == 0 && tot) atomicAdd(P.score, tot);
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int row = rbase + k;
+        if (row < m) P.c2r[n + (m - 1 - row)] = L[k];
+    }
+}
+
+template <typename T, int C>
+__global__ void __launch_bounds__(32, 1) comb_tile_kernel(const CombPair *__restrict__ pairs,
+                                                         const CombItem *__restrict__ items, int nitems, int *next,
+                                                         int *err, int one, int neg1) {
+    __shared__ __align__(16) TileShared<C> S;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int it = nitems;
+        if (lane == 0 && ld_relaxed(err) == kDevErrNone) it = atomicAdd(next, 1);
+        it = __shfl_sync(kFull, it, 0);
+        if (it >= nitems) return;
+        const CombItem I = items[it];
+        const CombPair P = pairs[I.pair];
+        switch (I.R) {
+            case 16: comb_tile_band<T, 16, C>(P, I, err, lane, one, neg1, S); break;
+            case 8: comb_tile_band<T, 8, C>(P, I, err, lane, one, neg1, S); break;
+            case 2: comb_tile_band<T, 2, C>(P, I, err, lane, one, neg1, S); break;
+            default: comb_tile_band<T, 4, C>(P, I, err, lane, one, neg1, S); break;
+        }
+    }
+}
+
 __global__ void invert_kernel(const int32_t *__restrict__ c2r, int size, int32_t *__restrict__ r2c, int rot,
                               int *err) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < size; i += gridDim.x * blockDim.x) {
@@ -235,6 +416,37 @@ int launch_comb_lone(const CombPair *d_pairs, const CombItem *d_items, int nitem
 }
 template int launch_comb_lone<uint8_t>(const CombPair *, const CombItem *, int, int *, int *, int, cudaStream_t);
 template int launch_comb_lone<int32_t>(const CombPair *, const CombItem *, int, int *, int *, int, cudaStream_t);
+
+int plan_tile_bands(int pair, int m, int R, std::vector<CombItem> &items) {
+    const int h = 32 * R;
+    const int bands = (m + h - 1) / h;
+    for (int i = 0; i < bands; ++i) items.push_back(CombItem{pair, i, i * h, R, i == bands - 1 ? 1 : 0});
+    return bands;
+}
+
+template <typename T>
+int launch_comb_tile(const CombPair *d_pairs, const CombItem *d_items, int nitems, int *d_next, int *d_err,
+                     int grid_warps, int C, cudaStream_t s) {
+    if (nitems <= 0) return SLCS_OK;
+    const int warps = grid_warps < nitems ? grid_warps : nitems;
+    if (C == 8)
+        comb_tile_kernel<T, 8><<<warps, 32, 0, s>>>(d_pairs, d_items, nitems, d_next, d_err, 1, -1);
+    else
+        comb_tile_kernel<T, 4><<<warps, 32, 0, s>>>(d_pairs, d_items, nitems, d_next, d_err, 1, -1);
+    SLCS_CUDA_TRY(cudaGetLastError());
+    return SLCS_OK;
+}
+template int launch_comb_tile<uint8_t>(const CombPair *, const CombItem *, int, int *, int *, int, int, cudaStream_t);
+template int launch_comb_tile<int32_t>(const CombPair *, const CombItem *, int, int *, int *, int, int, cudaStream_t);
+
+TileShape tile_shape_for(int rows, int band_rows, int lane_cols) {
+    if (lane_cols == 4 || lane_cols == 8) {
+        const bool given = band_rows == 64 || band_rows == 128 || band_rows == 256 || band_rows == 512;
+        return TileShape{given ? band_rows / 32 : kTileRows, lane_cols};
+    }
+    if (lane_cols != 0 || band_rows > 0) return TileShape{};   // one column per step / the band kernel's height
+    return rows <= kTileAutoMaxRows ? TileShape{kTileRows, kTileCols} : TileShape{};
+}
 
 int comb_resident_warps_sm(int num_sms) {
     int per_sm = 0;

@@ -20,6 +20,9 @@ struct slcs_pair_plan {
     int32_t *d_prog = nullptr, *d_c2r = nullptr;
     int *d_next = nullptr;
     int bands = 0, resident = 0;
+    bool tile = false;                       // the register-tile kernel (else the band kernel)
+    int tile_cols = 0;
+    unsigned long long *d_hand = nullptr;    // its hand-off words (n)
     const void *ba = nullptr, *bb = nullptr, *bscore = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // hybrid / bit
@@ -37,20 +40,27 @@ int wave_run(slcs_pair_plan *P, const uint8_t *d_a, const uint8_t *d_b, int32_t 
              cudaStream_t s, bool capturing) {
     if (P->ba != d_a || P->bb != d_b || P->bscore != d_score) {
         if (capturing) return fail(SLCS_ERR_ARG, "plan must run once on these buffers before capture");
-        CombPair hp{d_a, d_b, P->d_c2r, P->d_prog, d_score, P->m, P->n};
+        CombPair hp{d_a, d_b, P->d_c2r, P->d_prog, d_score, P->m, P->n, P->d_hand};
         SLCS_CUDA_TRY(cudaMemcpyAsync(P->d_pair, &hp, sizeof(hp), cudaMemcpyHostToDevice, s));
         SLCS_CUDA_TRY(cudaStreamSynchronize(s));
         P->ba = d_a;
         P->bb = d_b;
         P->bscore = d_score;
     }
-    SLCS_CUDA_TRY(cudaMemsetAsync(P->d_prog, 0, sizeof(int32_t) * std::max(P->bands, 1), s));
+    if (P->tile)
+        SLCS_CUDA_TRY(cudaMemsetAsync(P->d_hand, 0, sizeof(unsigned long long) * P->n, s));
+    else
+        SLCS_CUDA_TRY(cudaMemsetAsync(P->d_prog, 0, sizeof(int32_t) * std::max(P->bands, 1), s));
     SLCS_CUDA_TRY(cudaMemsetAsync(P->d_next, 0, sizeof(int), s));
     if (d_score) SLCS_CUDA_TRY(cudaMemsetAsync(d_score, 0, sizeof(int32_t), s));
     const unsigned fl = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     SLCS_CUDA_TRY(cudaEventRecordWithFlags(P->ev0, s, fl));
-    SLCS_TRY(launch_comb_lone<uint8_t>(P->d_pair, P->d_items, (int) P->items.size(), P->d_next, P->d_err,
-                                       P->resident, s));
+    if (P->tile)
+        SLCS_TRY(launch_comb_tile<uint8_t>(P->d_pair, P->d_items, (int) P->items.size(), P->d_next, P->d_err,
+                                           P->resident, P->tile_cols, s));
+    else
+        SLCS_TRY(launch_comb_lone<uint8_t>(P->d_pair, P->d_items, (int) P->items.size(), P->d_next, P->d_err,
+                                           P->resident, s));
     SLCS_CUDA_TRY(cudaEventRecordWithFlags(P->ev1, s, fl));
     SLCS_TRY(launch_invert(P->d_c2r, P->m + P->n, d_r2c, false, P->d_err, s));
     return SLCS_OK;
@@ -88,7 +98,7 @@ int slcs_pair_plan_destroy(slcs_pair_plan *P) {
     if (P->ev1) cudaEventDestroy(P->ev1);
     if (P->hyb) hybrid_plan_destroy(P->hyb);
     if (P->bit) bit_plan_destroy(P->bit);
-    void *ps[] = {P->d_err, P->d_items, P->d_pair, P->d_prog, P->d_c2r, P->d_next};
+    void *ps[] = {P->d_err, P->d_items, P->d_pair, P->d_prog, P->d_c2r, P->d_next, P->d_hand};
     for (void *p : ps) dfree(p, s);
     if (s) cudaStreamSynchronize(s);
     delete P;
@@ -116,8 +126,18 @@ int slcs_pair_plan_create(int m, int n, int kind, const slcs_opts *opts, slcs_pa
     if ((rc = dalloc(reinterpret_cast<void **>(&P->d_err), sizeof(int), s))) return bail(rc);
     if (cudaMemsetAsync(P->d_err, 0, sizeof(int), s) != cudaSuccess) return bail(fail(SLCS_ERR_CUDA, "memset"));
     if (kind == SLCS_ALGO_WAVEFRONT) {
-        const int R = (opts && opts->band_rows > 0) ? std::max(1, opts->band_rows / 32) : pick_rows_single(m);
-        P->bands = plan_bands(0, m, R, P->items);
+        const int band_rows = opts ? opts->band_rows : 0;
+        const TileShape ts = tile_shape_for(m, band_rows, opts ? opts->lane_cols : 0);
+        P->tile = ts.R > 0;
+        P->tile_cols = ts.C;
+        if (P->tile) {
+            P->bands = plan_tile_bands(0, m, ts.R, P->items);
+            if ((rc = dalloc(reinterpret_cast<void **>(&P->d_hand), sizeof(unsigned long long) * n, s)))
+                return bail(rc);
+        } else {
+            const int R = band_rows > 0 ? std::max(1, band_rows / 32) : pick_rows_single(m);
+            P->bands = plan_bands(0, m, R, P->items);
+        }
         P->resident = comb_resident_warps(E);
         if ((rc = dalloc(reinterpret_cast<void **>(&P->d_items), sizeof(CombItem) * P->items.size(), s)) ||
             (rc = dalloc(reinterpret_cast<void **>(&P->d_pair), sizeof(CombPair), s)) ||

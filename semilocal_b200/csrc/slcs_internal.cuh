@@ -105,6 +105,35 @@ __device__ __forceinline__ bool wait_at_least(const int *p, int need, int *err,
     return false;
 }
 
+// Hand-off words that carry a value and the tag of the band that wrote it in one 64-bit store: a reader that sees
+// the expected tag has the value, with no fence between them.
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long *p) {
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*const_cast<unsigned long long *>(p));
+    return r.load(cuda::memory_order_relaxed);
+}
+__device__ __forceinline__ void st_relaxed64(unsigned long long *p, unsigned long long v) {
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*p);
+    r.store(v, cuda::memory_order_relaxed);
+}
+// Until the hand-off word *p (already read into v) carries `tag` in its high half: re-reads it, polling without
+// sleeping first, bounded like wait_at_least (the error word is set when it gives up).  Data and tag travel in one
+// 64-bit store, so a word with the right tag is the right word.
+__device__ __forceinline__ bool wait_tag(const unsigned long long *p, unsigned long long &v, unsigned tag, int *err) {
+    if ((unsigned) (v >> 32) == tag) return true;
+    const unsigned long long t0 = global_ns();
+    for (long long it = 0; it < (1ll << 26); ++it) {
+        if (it >= kSpinPolls) __nanosleep(kSpinSleepNs);
+        v = ld_relaxed64(p);
+        if ((unsigned) (v >> 32) == tag) return true;
+        if ((it & 15) == 15) {
+            if (ld_relaxed(err) != kDevErrNone) return false;
+            if (global_ns() - t0 > kWaitLimitNs) break;
+        }
+    }
+    raise_error(err, kDevErrTimeout);
+    return false;
+}
+
 // ------------------------------------------------------------------------------------------------
 // per-device engine state: stream, error word, scratch arena
 // ------------------------------------------------------------------------------------------------
@@ -164,6 +193,7 @@ struct CombPair {
     int32_t *progress;    // per band: number of leading columns whose hand-off value is final
     int32_t *score;       // out (optional): global LLCS
     int m, n;
+    unsigned long long *hand;   // tile kernel only: n hand-off words (band tag << 32 | strand), zeroed per launch
 };
 
 struct CombItem {
@@ -185,6 +215,25 @@ int launch_comb(const CombPair *d_pairs, const CombItem *d_items, int nitems, in
 template <typename T>
 int launch_comb_lone(const CombPair *d_pairs, const CombItem *d_items, int nitems, int *d_next, int *d_err,
                      int grid_warps, cudaStream_t s);
+// Register-tile kernel for one pair alone on the device (comb.cu): a lane combs C columns of its R rows per step,
+// bands hand strands down through the pair's `hand` words (zeroed before every launch).  Bands come from
+// plan_tile_bands (one height for all, the last padded with rows that never swap); R in {2, 4, 8, 16}, C in {4, 8}.
+constexpr int kTileRows = 8;                  // default tile: kTileRows x kTileCols cells per lane and step
+constexpr int kTileCols = 4;
+constexpr int kTileAutoMaxRows = 1 << 17;     // lone pairs up to this many rows take the tile kernel by default
+int plan_tile_bands(int pair, int m, int R, std::vector<CombItem> &items);
+template <typename T>
+int launch_comb_tile(const CombPair *d_pairs, const CombItem *d_items, int nitems, int *d_next, int *d_err,
+                     int grid_warps, int C, cudaStream_t s);
+// The tile a lone pair of `rows` rows is combed with; R = 0: the band kernel.  lane_cols is the caller's choice
+// (slcs_opts.lane_cols): 4 or 8 = the tile kernel with that width, band_rows 64..512 giving its height (else
+// kTileRows); 1 = the band kernel; 0 = automatic: the band kernel when band_rows is given, else the tile kernel up
+// to kTileAutoMaxRows rows, where its few bands leave the SMs short of warps, and the band kernel above, which
+// issues fewer instructions per cell.
+struct TileShape {
+    int R = 0, C = 0;
+};
+TileShape tile_shape_for(int rows, int band_rows, int lane_cols);
 // Warps that fit on the device at once for the combing kernel.
 int comb_resident_warps(Engine *E);
 int comb_resident_warps_sm(int num_sms);

@@ -78,3 +78,43 @@ def test_batch_vs_single(engine, oracle):
         assert np.array_equal(res0[i], exp), i
         assert np.array_equal(res1[i], exp), i
         assert sc0[i] == sc1[i] == oracle.global_score(exp, len(a), len(b)), i
+
+
+@pytest.mark.parametrize("lane_cols", [4, 8])
+@pytest.mark.parametrize("band_rows", [64, 128, 256, 512])
+def test_tile_kernel_shapes(engine, oracle, band_rows, lane_cols):
+    """The register-tile kernel of lone pairs: ragged widths (not multiples of 4 or 32), one band, a padded last
+    band, fewer columns than lanes, and many bands; against the oracle, braids and scores."""
+    rng = np.random.default_rng(band_rows + 7)
+    shapes = [(1, 1), (1, 37), (37, 1), (5, 3), (31, 33), (band_rows, 4), (band_rows + 1, 129), (1000, 777),
+              (777, 1000), (2049, 63), (63, 2049), (3 * band_rows - 5, 1023), (4096, 4099)]
+    for m, n in shapes:
+        a, b = _rand(rng, m, 4), _rand(rng, n, 4)
+        r2c, score = engine.comb(a, b, algo=engine.ALGO_WAVEFRONT, band_rows=band_rows, lane_cols=lane_cols)
+        exp = oracle.comb_antidiag(a, b, 4)
+        assert np.array_equal(r2c, exp), (m, n)
+        assert score == oracle.global_score(exp, m, n), (m, n)
+
+
+def test_tile_kernel_wide_alphabet_and_plan(engine, oracle):
+    """int32 symbols through the tile kernel, and a reusable plan (graph replays) on the 8192 pair."""
+    import torch
+    rng = np.random.default_rng(12)
+    for m, n, alpha in [(300, 201, 150), (123, 457, 1000), (640, 64, 100000)]:
+        a = rng.integers(-alpha, alpha, m).astype(np.int32)
+        b = rng.integers(-alpha, alpha, n).astype(np.int32)
+        for lc in (4, 8):
+            r2c, _ = engine.comb(a, b, algo=engine.ALGO_WAVEFRONT, lane_cols=lc)
+            assert np.array_equal(r2c, oracle.comb_rowmajor(a, b)), (m, n, alpha, lc)
+    a, b = gen.plain_pair(8192, seed=1)
+    exp = oracle.comb_antidiag(a, b, 8)
+    da, db = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    r2c = torch.empty(16384, dtype=torch.int32, device="cuda")
+    sc = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pl = engine.PairPlan(8192, 8192, engine.ALGO_WAVEFRONT, lane_cols=4)
+    for g in (False, True, True, True):
+        pl.run(da.data_ptr(), db.data_ptr(), r2c.data_ptr(), sc.data_ptr(), g)
+        pl.check()
+        assert np.array_equal(r2c.cpu().numpy(), exp), g
+        assert int(sc.item()) == oracle.global_score(exp, 8192, 8192), g
+    pl.close()
