@@ -112,6 +112,12 @@ int slcs_lcs_u8(const uint8_t *a, int m, const uint8_t *b, int n, int32_t *score
  * (:598-663) for symbols < 2; unlike the reference any lengths are accepted. */
 int slcs_bitcomb_llcs_u8(const uint8_t *a, int m, const uint8_t *b, int n, int32_t *score);
 int slcs_bitcomb_llcs_u8_dev(const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_score, void *stream);
+/* LLCS by the bit-vector recurrence V' = (V + (V & match)) | (V & ~match) over one string's symbols (Allison-Dix,
+ * Hyyro), the carry running through the whole vector; symbols must be < 4.  Replaces lllcs_hyyro::hyyro_magic and
+ * hyyro_magic_mpi_with_precalc (R:prefix_lcs/bitwise/transposition_network_binary_alphabet.h:787-914, which build
+ * the vector over their `b` and loop over `a`; the engine puts the vector over the longer string). */
+int slcs_hyyro_llcs_u8(const uint8_t *a, int m, const uint8_t *b, int n, int32_t *score);
+int slcs_hyyro_llcs_u8_dev(const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_score, void *stream);
 
 /* ---- unit-Monge braid multiplication (steady ant) -------------------------------------------- */
 /* r = p (.) q for n x n permutations given as row->col maps.
@@ -222,12 +228,13 @@ int slcs_batch_info(slcs_batch *bt, int64_t *cells, int32_t *launches, int64_t *
 int slcs_batch_destroy(slcs_batch *bt);
 
 /* ---- single-pair plans (device-resident, reusable, graph-capturable) -------------------------- */
-/* kind: SLCS_ALGO_WAVEFRONT, SLCS_ALGO_HYBRID (braid + score) or SLCS_PLAN_BITPARALLEL (score only).
+/* kind: SLCS_ALGO_WAVEFRONT, SLCS_ALGO_HYBRID (braid + score), SLCS_PLAN_BITPARALLEL or SLCS_PLAN_HYYRO (score only).
  * create() plans and allocates everything for an m x n pair; run() launches kernels on `stream` (uint8
  * device strings; with use_graph != 0 the launch sequence is captured once per buffer set and replayed);
  * check() waits and reports the device error word; kernel_ms() is the device time of the last run's
  * combing kernel (CUDA events on the run's stream). */
 #define SLCS_PLAN_BITPARALLEL 3
+#define SLCS_PLAN_HYYRO 4
 typedef struct slcs_pair_plan slcs_pair_plan;
 int slcs_pair_plan_create(int m, int n, int kind, const slcs_opts *opts, slcs_pair_plan **out);
 int slcs_pair_plan_run(slcs_pair_plan *pl, const uint8_t *d_a, const uint8_t *d_b, int32_t *d_row_to_col,

@@ -68,6 +68,7 @@ def lib():
             L.slo_bit_llcs_nary_u64.argtypes = [_u64p, ctypes.c_int, _u64p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
             L.slo_bit_llcs_binary_u64.argtypes = [_u64p, ctypes.c_int, _u64p, ctypes.c_int, ctypes.c_int]
             L.slo_comb_score.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int]
+            L.slo_hyyro_llcs.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int]
             L.slo_duplicate_search.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_double, _i32p, _i32p,
                                                _f64p, ctypes.c_int]
             L.slo_duplicate_search_sparse.argtypes = L.slo_duplicate_search.argtypes
@@ -103,6 +104,7 @@ def ref():
                 R.ref_lcs_by_semilocal.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int]
                 R.ref_bit_nary_u64.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
                 R.ref_bit_binary_u64.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int]
+                R.ref_hyyro_u64.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int]
                 _ref = R
     return _ref
 
@@ -243,6 +245,12 @@ def bit_llcs_binary(a, b) -> int:
     return int(lib().slo_bit_llcs_binary_u64(_pu(ar), len(ar), _pu(be), len(be), len(a)))
 
 
+def hyyro_llcs(a, b) -> int:
+    """Bit-vector LLCS (Allison-Dix / Hyyro recurrence) over 64-bit words of `a`, looping over `b`."""
+    a, b = _i32(a), _i32(b)
+    return int(lib().slo_hyyro_llcs(_p(a), len(a), _p(b), len(b)))
+
+
 def comb_score(a, b, threads: int = 1) -> int:
     a, b = _i32(a), _i32(b)
     return int(lib().slo_comb_score(_p(a), len(a), _p(b), len(b), threads))
@@ -326,6 +334,14 @@ def ref_bit_nary(a, b, alphabet: int = 4, threads: int = 1) -> int:
     R = ref()
     a, b = _i32(a), _i32(b)
     return int(R.ref_bit_nary_u64(_p(a), len(a), _p(b), len(b), alphabet, threads))
+
+
+def ref_hyyro(vec, seq, threads: int = 1) -> int:
+    """The reference's lllcs_hyyro (bit vector over `vec`, loop over `seq`; threads > 1: its anti-diagonal form,
+    which wants len(seq) > words of vec)."""
+    R = ref()
+    vec, seq = _i32(vec), _i32(seq)
+    return int(R.ref_hyyro_u64(_p(vec), len(vec), _p(seq), len(seq), threads))
 
 
 def ref_bit_binary(a, b, threads: int = 1) -> int:

@@ -252,6 +252,23 @@ int ref_bit_binary_u64(const int *a, int m, const int *b, int n, int threads) {
     return res;
 }
 
+// lllcs_hyyro::preprocess + hyyro_magic<uint64_t> (threads == 1) or hyyro_magic_mpi_with_precalc (threads > 1)
+// (transposition_network_binary_alphabet.h:749-914): the bit vector runs over `vec` (its lookup tables), the loop over
+// `seq`.  The anti-diagonal form assumes more symbols in `seq` than words in `vec`.
+int ref_hyyro_u64(const int *vec, int nv, const int *seq, int ns, int threads) {
+    if (nv == 0 || ns == 0) return 0;
+    std::unordered_set<int> alpha(vec, vec + nv);
+    alpha.insert(seq, seq + ns);
+    std::unordered_map<int, uint64_t *> lookup;
+    lllcs_hyyro::preprocess<uint64_t>(vec, nv, alpha, lookup);
+    const int words = (nv + 63) / 64;
+    std::vector<int> sv(seq, seq + ns);
+    int res = threads > 1 ? lllcs_hyyro::hyyro_magic_mpi_with_precalc<uint64_t>(sv.data(), ns, words, lookup, threads)
+                          : lllcs_hyyro::hyyro_magic<uint64_t>(sv.data(), ns, words, lookup);
+    for (auto &kv : lookup) delete[] kv.second;
+    return res;
+}
+
 int ref_available(void) { return 1; }
 
 }  // extern "C"

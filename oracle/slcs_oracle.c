@@ -715,4 +715,42 @@ int slo_comb_score(const int32_t *a, int m, const int32_t *b, int n, int threads
     return s;
 }
 
+/* Bit-vector LLCS (R:prefix_lcs/bitwise/transposition_network_binary_alphabet.h:749-830, lllcs_hyyro::preprocess and
+ * hyyro_magic): V over the symbols of `a` (bit i = a[i], 64-bit words), all ones; for every symbol c of b:
+ * p = match(c) & V; V = (V ^ p) | (V + p + carry), the carry running from word to word; the score is the number
+ * of zero bits of V over the real positions (padding bits never take a match, so they stay 1). */
+int slo_hyyro_llcs(const int32_t *a, int m, const int32_t *b, int n) {
+    if (m == 0 || n == 0) return 0;
+    const int W = (m + 63) / 64;
+    uint64_t *V = (uint64_t *) malloc(sizeof(uint64_t) * W);
+    uint64_t *Mt = (uint64_t *) calloc((size_t) W, sizeof(uint64_t));
+    for (int w = 0; w < W; ++w) V[w] = ~0ull;
+    for (int j = 0; j < n; ++j) {
+        for (int w = 0; w < W; ++w) {
+            uint64_t x = 0;
+            for (int i = 0; i < 64 && 64 * w + i < m; ++i)
+                if (a[64 * w + i] == b[j]) x |= 1ull << i;
+            Mt[w] = x;
+        }
+        uint64_t carry = 0;
+        for (int w = 0; w < W; ++w) {
+            const uint64_t v = V[w], p = Mt[w] & v;
+            const uint64_t s1 = v + p;
+            const uint64_t c1 = s1 < v;
+            const uint64_t s2 = s1 + carry;
+            const uint64_t c2 = s2 < s1;
+            V[w] = (v ^ p) | s2;
+            carry = c1 | c2;
+        }
+    }
+    int zeros = 0;
+    for (int w = 0; w < W; ++w) {
+        const int bits = (64 * (w + 1) <= m) ? 64 : m - 64 * w;
+        for (int i = 0; i < bits; ++i) zeros += !((V[w] >> i) & 1ull);
+    }
+    free(V);
+    free(Mt);
+    return zeros;
+}
+
 int slo_version(void) { return 1; }

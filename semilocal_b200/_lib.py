@@ -20,6 +20,7 @@ ERRORS = {
 
 ALGO_AUTO, ALGO_WAVEFRONT, ALGO_HYBRID = 0, 1, 2
 PLAN_BITPARALLEL = 3
+PLAN_HYYRO = 4
 Q_GLOBAL, Q_STRING_SUBSTRING, Q_PREFIX_SUFFIX, Q_SUFFIX_PREFIX, Q_SUBSTRING_STRING, Q_MATRIX = range(6)
 
 
@@ -90,6 +91,8 @@ SIGNATURES = {
     "slcs_lcs_u8": [_u8p, _int, _u8p, _int, _i32p],
     "slcs_bitcomb_llcs_u8": [_u8p, _int, _u8p, _int, _i32p],
     "slcs_bitcomb_llcs_u8_dev": [_vp, _int, _vp, _int, _vp, _vp],
+    "slcs_hyyro_llcs_u8": [_u8p, _int, _u8p, _int, _i32p],
+    "slcs_hyyro_llcs_u8_dev": [_vp, _int, _vp, _int, _vp, _vp],
     "slcs_steady_ant": [_i32p, _i32p, _int, _i32p, _optp],
     "slcs_steady_ant_dev": [_vp, _vp, _int, _vp, _optp, _vp],
     "slcs_sa_plan_create": [_int, ctypes.POINTER(_vp)],

@@ -106,6 +106,14 @@ def bitcomb_llcs(a, b) -> int:
     return int(s.value)
 
 
+def hyyro_llcs(a, b) -> int:
+    """LLCS by the bit-vector (Hyyro) kernel (symbols < 4)."""
+    au, bu = _u8(a), _u8(b)
+    s = ctypes.c_int32(0)
+    check(lib().slcs_hyyro_llcs_u8(_p(au, _u8p), len(au), _p(bu, _u8p), len(bu), ctypes.byref(s)))
+    return int(s.value)
+
+
 def steady_ant(p, q, sa_cutoff: int = 0) -> np.ndarray:
     """Unit-Monge product r = p (.) q of two permutations (row->col int32)."""
     p = np.ascontiguousarray(p, dtype=np.int32)
@@ -282,10 +290,11 @@ def concat_pairs(pairs):
 
 class PairPlan:
     """A reusable single-pair plan on device buffers (include/slcs.h: slcs_pair_plan_*): kind is ALGO_WAVEFRONT,
-    ALGO_HYBRID or PLAN_BITPARALLEL.  run() takes device pointers (ints) and a stream handle."""
+    ALGO_HYBRID, PLAN_BITPARALLEL or PLAN_HYYRO.  run() takes device pointers (ints) and a stream handle."""
 
     def __init__(self, m: int, n: int, kind: int, tile: int = 0, band_rows: int = 0, lane_cols: int = 0):
-        o = _lib.opts(kind if kind != _lib.PLAN_BITPARALLEL else 0, tile, tile, band_rows, 0, lane_cols)
+        o = _lib.opts(kind if kind not in (_lib.PLAN_BITPARALLEL, _lib.PLAN_HYYRO) else 0, tile, tile, band_rows, 0,
+                      lane_cols)
         h = ctypes.c_void_p()
         check(lib().slcs_pair_plan_create(m, n, kind, ctypes.byref(o), ctypes.byref(h)))
         self.h, self.m, self.n, self.kind = h, m, n, kind

@@ -28,6 +28,7 @@ struct slcs_pair_plan {
     // hybrid / bit
     HybridPlan *hyb = nullptr;
     BitPlan *bit = nullptr;
+    HyyroPlan *hy = nullptr;
     // graph
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -78,6 +79,7 @@ int plan_run(slcs_pair_plan *P, const uint8_t *d_a, const uint8_t *d_b, int32_t 
         if (d_score) SLCS_TRY(hybrid_score(P->hyb, d_score, s));
         return SLCS_OK;
     }
+    if (P->kind == SLCS_PLAN_HYYRO) return hyyro_plan_run(P->hy, d_a, d_b, d_score, P->d_err, s, capturing);
     return bit_plan_run(P->bit, d_a, d_b, d_score, P->d_err, s, capturing);
 }
 
@@ -98,6 +100,7 @@ int slcs_pair_plan_destroy(slcs_pair_plan *P) {
     if (P->ev1) cudaEventDestroy(P->ev1);
     if (P->hyb) hybrid_plan_destroy(P->hyb);
     if (P->bit) bit_plan_destroy(P->bit);
+    if (P->hy) hyyro_plan_destroy(P->hy);
     void *ps[] = {P->d_err, P->d_items, P->d_pair, P->d_prog, P->d_c2r, P->d_next, P->d_hand};
     for (void *p : ps) dfree(p, s);
     if (s) cudaStreamSynchronize(s);
@@ -107,7 +110,8 @@ int slcs_pair_plan_destroy(slcs_pair_plan *P) {
 
 int slcs_pair_plan_create(int m, int n, int kind, const slcs_opts *opts, slcs_pair_plan **out) {
     if (!out || m < 1 || n < 1 || (long long) m + n >= (1ll << 30)) return fail(SLCS_ERR_ARG, "bad plan arguments");
-    if (kind != SLCS_ALGO_WAVEFRONT && kind != SLCS_ALGO_HYBRID && kind != SLCS_PLAN_BITPARALLEL)
+    if (kind != SLCS_ALGO_WAVEFRONT && kind != SLCS_ALGO_HYBRID && kind != SLCS_PLAN_BITPARALLEL &&
+        kind != SLCS_PLAN_HYYRO)
         return fail(SLCS_ERR_ARG, "unknown plan kind");
     *out = nullptr;
     Engine *E;
@@ -155,7 +159,11 @@ int slcs_pair_plan_create(int m, int n, int kind, const slcs_opts *opts, slcs_pa
         if ((rc = hybrid_plan_create(m, n, tr, tc, E, s, &P->hyb)) || (rc = hybrid_enable_timing(P->hyb)))
             return bail(rc);
     } else {
-        if ((rc = bit_plan_create(E, m, n, s, &P->bit))) return bail(rc);
+        if (kind == SLCS_PLAN_HYYRO) {
+            if ((rc = hyyro_plan_create(E, m, n, s, &P->hy))) return bail(rc);
+        } else if ((rc = bit_plan_create(E, m, n, s, &P->bit))) {
+            return bail(rc);
+        }
     }
     if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(SLCS_ERR_CUDA, "plan setup failed"));
     *out = P;
@@ -165,8 +173,9 @@ int slcs_pair_plan_create(int m, int n, int kind, const slcs_opts *opts, slcs_pa
 int slcs_pair_plan_run(slcs_pair_plan *P, const uint8_t *d_a, const uint8_t *d_b, int32_t *d_row_to_col,
                        int32_t *d_score, int use_graph, void *stream) {
     if (!P || !d_a || !d_b) return fail(SLCS_ERR_ARG, "NULL argument");
-    if (P->kind != SLCS_PLAN_BITPARALLEL && !d_row_to_col) return fail(SLCS_ERR_ARG, "NULL row_to_col");
-    if (P->kind == SLCS_PLAN_BITPARALLEL && !d_score) return fail(SLCS_ERR_ARG, "NULL score");
+    const bool score_only = P->kind == SLCS_PLAN_BITPARALLEL || P->kind == SLCS_PLAN_HYYRO;
+    if (!score_only && !d_row_to_col) return fail(SLCS_ERR_ARG, "NULL row_to_col");
+    if (score_only && !d_score) return fail(SLCS_ERR_ARG, "NULL score");
     SLCS_CUDA_TRY(cudaSetDevice(P->device));
     Engine *E;
     SLCS_TRY(engine(&E));
@@ -213,6 +222,7 @@ int slcs_pair_plan_kernel_ms(slcs_pair_plan *P, float *ms) {
     if (!P || !ms) return fail(SLCS_ERR_ARG, "NULL argument");
     if (P->kind == SLCS_ALGO_HYBRID) return hybrid_comb_ms(P->hyb, ms);
     if (P->kind == SLCS_PLAN_BITPARALLEL) return bit_plan_kernel_ms(P->bit, ms);
+    if (P->kind == SLCS_PLAN_HYYRO) return hyyro_plan_kernel_ms(P->hy, ms);
     SLCS_CUDA_TRY(cudaEventSynchronize(P->ev1));
     SLCS_CUDA_TRY(cudaEventElapsedTime(ms, P->ev0, P->ev1));
     return SLCS_OK;
@@ -221,7 +231,7 @@ int slcs_pair_plan_kernel_ms(slcs_pair_plan *P, float *ms) {
 int slcs_pair_plan_launches(slcs_pair_plan *P, int32_t *launches) {
     if (!P || !launches) return fail(SLCS_ERR_ARG, "NULL argument");
     if (P->kind == SLCS_ALGO_HYBRID) *launches = hybrid_launches(P->hyb) + 1;
-    else if (P->kind == SLCS_PLAN_BITPARALLEL) *launches = 3;
+    else if (P->kind == SLCS_PLAN_BITPARALLEL || P->kind == SLCS_PLAN_HYYRO) *launches = 3;
     else *launches = 2;
     return SLCS_OK;
 }

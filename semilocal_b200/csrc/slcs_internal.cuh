@@ -302,6 +302,17 @@ int bit_plan_kernel_ms(BitPlan *B, float *ms);
 void bit_plan_destroy(BitPlan *B);
 
 // ------------------------------------------------------------------------------------------------
+// bit-vector LLCS, Hyyro recurrence (hyyro.cu)
+// ------------------------------------------------------------------------------------------------
+struct HyyroPlan;
+int hyyro_plan_create(Engine *E, int m, int n, cudaStream_t s, HyyroPlan **out);
+int hyyro_plan_run(HyyroPlan *H, const uint8_t *d_a, const uint8_t *d_b, int32_t *d_score, int *d_err,
+                   cudaStream_t s, bool capturing);
+int hyyro_plan_kernel_ms(HyyroPlan *H, float *ms);
+void hyyro_plan_destroy(HyyroPlan *H);
+int hyyro_dev(Engine *E, const uint8_t *d_a, int m, const uint8_t *d_b, int n, int32_t *d_score, cudaStream_t s);
+
+// ------------------------------------------------------------------------------------------------
 // scores (scores.cu)
 // ------------------------------------------------------------------------------------------------
 // Maps a query to the semi-local matrix entry H(i, j) it reads and the offset added to it; ok = false for

@@ -82,6 +82,7 @@ def test_sizes_beyond_the_limit_are_rejected_before_device_work():
         "slcs_window_scores": lambda: L.slcs_window_scores(p, big, big, 5, p),
         "slcs_window_scores_dev": lambda: L.slcs_window_scores_dev(p, p, big, big, 5, p, None),
         "slcs_bitcomb_llcs_u8_dev": lambda: L.slcs_bitcomb_llcs_u8_dev(p, big, p, big, p, None),
+        "slcs_hyyro_llcs_u8_dev": lambda: L.slcs_hyyro_llcs_u8_dev(p, big, p, big, p, None),
         "slcs_staggered_glue": lambda: L.slcs_staggered_glue(p, big, big, p, big, big, 1, p),
         "slcs_steady_ant": lambda: L.slcs_steady_ant(p, p, 1 << 30, p, None),
         "slcs_comb_i32": lambda: L.slcs_comb_i32(p, big, p, big, p, None, None, None),

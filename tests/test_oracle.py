@@ -74,6 +74,26 @@ ref_only = pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(__
                               reason="reference library oracle/_ref not built (needs the reference sources)")
 
 
+def test_hyyro_vs_dp(oracle):
+    """The bit-vector (Hyyro) restatement against the DP on ragged lengths (words of 64 rows, partial last words)."""
+    rng = np.random.default_rng(9)
+    for m, n in [(0, 5), (5, 0), (1, 1), (63, 64), (64, 65), (65, 63), (200, 333), (1000, 17)]:
+        a, b = _rand(rng, m, 4), _rand(rng, n, 4)
+        assert oracle.hyyro_llcs(a, b) == oracle.lcs_dp(a, b), (m, n)
+
+
+@ref_only
+def test_hyyro_matches_reference(oracle):
+    """Pin: the restatement equals the reference's own lllcs_hyyro (its sequential and anti-diagonal forms)."""
+    rng = np.random.default_rng(10)
+    for m, n in [(1, 1), (63, 200), (64, 64), (130, 500), (700, 900), (2000, 300)]:
+        a, b = _rand(rng, m, 4), _rand(rng, n, 4)
+        exp = oracle.hyyro_llcs(a, b)
+        assert oracle.ref_hyyro(a, b) == exp, (m, n)
+        if n > (m + 63) // 64:
+            assert oracle.ref_hyyro(a, b, 4) == exp, (m, n)
+
+
 @ref_only
 def test_restatement_matches_reference(oracle):
     rng = np.random.default_rng(6)
