@@ -42,6 +42,9 @@ COMB_PIPE_SPLIT = {"alu_pct_of_peak": 60.6, "fma_pct_of_peak": 31.6, "issue_pct"
 SM_COUNT = 148
 # bit-parallel ops per cell: 17 ops per step, 2S - 1 steps per S x S word cell, S = 32 symbols per 64-bit word
 BIT_OPS_PER_CELL = 17 * (2 * 32 - 1) / (32 * 32)
+# the bit-vector (Hyyro) kernel: 55.25 warp instructions per step of a lane's 32 rows x 4 columns (ncu instruction
+# count of one band, 1024 x 262144: 3.62e6 instructions over 65567 steps), i.e. lane-ops per cell
+HY_OPS_PER_CELL = 55.25 / 128
 DIGESTS_PATH = os.path.join(ROOT, "tests", "golden", "headline_digests.json")
 
 
@@ -141,9 +144,9 @@ def check_against_reference(braids, scores, ms, ns, shard):
                          "the reference compiled from its sources (tests/golden/headline_digests.json)"}
 
 
-def check_pair_2p20(braids, bit_score, m, n):
+def check_pair_2p20(braids, bit_scores, m, n):
     """The 2^20 pair's braids against the digest of the reference's OpenMPHybridIterative braid and its bit
-    score against the reference braid's global score (tests/golden/headline_digests.json)."""
+    scores against the reference braid's global score (tests/golden/headline_digests.json)."""
     import hashlib
     try:
         with open(DIGESTS_PATH) as f:
@@ -153,7 +156,8 @@ def check_pair_2p20(braids, bit_score, m, n):
     out = {name + "_bit_exact_vs_reference":
            hashlib.sha256(np.ascontiguousarray(r, dtype="<i4").tobytes()).hexdigest() == ref["sha256"]
            for name, r in braids.items()}
-    out["bit_parallel_score_equals_reference"] = int(bit_score) == ref["global_score"] and (m, n) == (ref["m"], ref["n"])
+    for name, sc in bit_scores.items():
+        out[name + "_score_equals_reference"] = int(sc) == ref["global_score"] and (m, n) == (ref["m"], ref["n"])
     out["reference"] = "OpenMPHybridIterative<int,false>(threads, 4096, 4096), the reference compiled from its sources"
     return out
 
@@ -512,9 +516,11 @@ def run_suite(torch, S, peak_cells, peaks):
     # the hybrid with the configuration's 4096 x 4096 tiles, and with 65536 x 65536 tiles (the reference's own
     # OpenMPHybridIterative(threads, 65536, 65536): 256 tiles, 8 glue levels instead of 16)
     for name, kind, tile in (("hybrid_tiles_4096", S.ALGO_HYBRID, 4096), ("hybrid_tiles_65536", S.ALGO_HYBRID, 65536),
-                             ("wavefront", S.ALGO_WAVEFRONT, 0), ("bit_parallel", S.PLAN_BITPARALLEL, 0)):
+                             ("wavefront", S.ALGO_WAVEFRONT, 0), ("bit_parallel", S.PLAN_BITPARALLEL, 0),
+                             ("bit_vector_hyyro", S.PLAN_HYYRO, 0)):
+        score_only = kind in (S.PLAN_BITPARALLEL, S.PLAN_HYYRO)
         pl = S.PairPlan(m, n, kind, tile=tile)
-        r2 = torch.empty(m + n, dtype=torch.int32, device="cuda") if kind != S.PLAN_BITPARALLEL else None
+        r2 = torch.empty(m + n, dtype=torch.int32, device="cuda") if not score_only else None
         sc2 = torch.zeros(1, dtype=torch.int32, device="cuda")
         fn = lambda: pl.run(da.data_ptr(), db.data_ptr(), r2.data_ptr() if r2 is not None else None,
                             sc2.data_ptr(), True, sh)
@@ -523,18 +529,20 @@ def run_suite(torch, S, peak_cells, peaks):
         kms = pl.kernel_ms()
         ent = {"gpu_ms": round(ms, 2), "gcups": round(m * n / ms / 1e6, 1), "score": int(sc2.item()),
                "comb_kernel_ms": round(kms, 2), "launches": pl.launches()}
-        if kind != S.PLAN_BITPARALLEL:
+        if not score_only:
             # whole run (tiles + glue for the hybrid) and combing kernel alone, against the cell-mix probe
             ent["roofline_frac_whole_run"] = round(m * n / (ms * 1e-3) / peak_cells, 4)
             ent["roofline_frac_comb_kernel"] = round(m * n / (kms * 1e-3) / peak_cells, 4)
             braids[name] = r2.cpu().numpy()
         else:
-            # the bit-parallel convention: 17 ops per step of a 32-symbol word cell, 2S - 1 = 63 steps per
-            # S^2 = 1024 cells (R:prefix_lcs/bitwise/transposition_network_binary_alphabet.h:351-370), against the
-            # SM issue ceiling (one lane-op per issue slot) at the sampled clock
-            ops = BIT_OPS_PER_CELL * m * n
+            # ops per cell: the braid-in-bits convention, 17 ops per step of a 32-symbol word cell, 2S - 1 = 63
+            # steps per S^2 = 1024 cells (R:prefix_lcs/bitwise/transposition_network_binary_alphabet.h:351-370);
+            # the bit-vector kernel's own measured instruction count; against the SM issue ceiling (one lane-op per
+            # issue slot) at the sampled clock
+            opc = BIT_OPS_PER_CELL if kind == S.PLAN_BITPARALLEL else HY_OPS_PER_CELL
+            ops = opc * m * n
             ceiling = issue_ceiling_gops({}) * 1e9
-            ent["int_ops_per_cell"] = round(BIT_OPS_PER_CELL, 4)
+            ent["int_ops_per_cell"] = round(opc, 4)
             ent["roofline_frac_whole_run"] = round(ops / (ms * 1e-3) / ceiling, 4)
             ent["roofline_frac_kernel"] = round(ops / (kms * 1e-3) / ceiling, 4)
             ent["roofline_peak"] = "SM issue ceiling, 148 SM x 4 SMSP x 32 lanes x 1965 MHz"
@@ -545,8 +553,8 @@ def run_suite(torch, S, peak_cells, peaks):
     res["hybrid_equals_wavefront"] = bool(np.array_equal(braids["hybrid_tiles_4096"], braids["wavefront"]) and
                                           np.array_equal(braids["hybrid_tiles_65536"], braids["wavefront"]))
     res["scores_agree"] = len({res[k]["score"] for k in ("hybrid_tiles_4096", "hybrid_tiles_65536", "wavefront",
-                                                           "bit_parallel")}) == 1
-    res["parity"] = check_pair_2p20(braids, res["bit_parallel"]["score"], m, n)
+                                                           "bit_parallel", "bit_vector_hyyro")}) == 1
+    res["parity"] = check_pair_2p20(braids, {k: res[k]["score"] for k in ("bit_parallel", "bit_vector_hyyro")}, m, n)
     # the reference's hybrid on a bounded sample: the leading 2^16 x 2^16 corner of the same pair
     sa, sb = a[:1 << 16].astype(np.int32), b[:1 << 16].astype(np.int32)
     if use_ref:

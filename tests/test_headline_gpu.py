@@ -95,5 +95,7 @@ def test_bit_2p20_vs_reference(engine, digests, pair_2p20):
         ta, tb = tb, ta
     assert (len(ta), len(tb)) == (ref["len_a"], ref["len_b"])
     assert engine.bitcomb_llcs(ta, tb) == ref["llcs"]
+    assert engine.hyyro_llcs(ta, tb) == ref["llcs"]
     # the untrimmed pair (outside the reference routine's domain) against the reference braid's score
     assert engine.bitcomb_llcs(a, b) == digests["hybrid_2p20"]["global_score"]
+    assert engine.hyyro_llcs(a, b) == digests["hybrid_2p20"]["global_score"]
