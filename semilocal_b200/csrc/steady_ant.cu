@@ -822,6 +822,8 @@ constexpr int kBandThreads = 256;
 constexpr int kBandSub = kBand / (kBandThreads / 32);   // rows per warp sub-band
 constexpr int kBandWalk = kBand / kBandThreads;         // rows per thread walk
 constexpr int kBandYCap = 12288;   // columns a band stages in shared memory
+// block table of a wider band, in the same space: 2 + 4 bytes per block and 2 per own row (kBand rows)
+constexpr int kWideMaxBlocks = (4 * kBandYCap - 2 * 4096 - 2) / 6;
 constexpr unsigned kHiBit = 1u << 30;
 constexpr int kRowHistSmemMax = 200 * 1024;   // block-table width limit of sa_rowhist_kernel's histogram
 constexpr int kValMask = (1 << 30) - 1;
@@ -1101,13 +1103,35 @@ struct BandShared {
     int nq;
 };
 
-// Column points of the node: from shared memory when the band's column range was staged, else from global.
+// Column points of the node: from shared memory when the band's column range was staged, else from global memory
+// with, in shared memory, a table over blocks of B columns of [clo, cend) (built by build_wide_tables):
+//   stat[b]  columns of block b whose point raises delta for every row of the band (hi points of rows < R0, lo
+//            points of rows >= R1);
+//   bend[b]  end in dyn of block b's points of the band's own rows [R0, R1) (block b: dyn[bend[b-1] .. bend[b]));
+//   dyn[e]   such a point: its row offset i (row R0 + i) and hi bit (bit 15), which raises delta in row R iff
+//            hi ? R0 + i < R : R0 + i >= R.
+// A block's raising count for row R is then stat[b] plus a scan of its few own-row points: a search skips whole
+// blocks and reads columns from global memory only in the block where it ends.
 struct YView {
     const int32_t *s;   // shared copy of columns [clo, clo + ny)
     const int32_t *g;   // the node's columns in global memory
     int clo;
     bool in_smem;
+    const uint16_t *stat;
+    const int32_t *bend;
+    const uint16_t *dyn;
+    int B, nblk, R0;
     __device__ __forceinline__ int operator()(int c) const { return in_smem ? s[c - clo] : __ldg(g + c); }
+    // raising columns of full block b for row R
+    __device__ __forceinline__ int block_count(int b, int R) const {
+        int cnt = stat[b];
+        for (int e = b ? bend[b - 1] : 0, ee = bend[b]; e < ee; ++e) {
+            const int d = dyn[e];
+            const int r = R0 + (d & 0x0fff);
+            cnt += (d & 0x8000) ? (r < R) : (r >= R);
+        }
+        return cnt;
+    }
 };
 
 // warp-wide: rows i in [i0, i1) of the band whose point raises delta when moving up past it at column c
@@ -1153,10 +1177,11 @@ __device__ __forceinline__ int ballot_search_grow(int from, int end, int need, i
 }
 
 // warp-wide, columns in global memory (a band whose column range was too wide to stage): one past the need-th
-// column g in [from, end) whose point raises delta in row R, `none` if there are fewer.  Rounds of 512 columns, each
+// column g in [from, end) whose point raises delta in row R, `none` if there are fewer (need then reduced by the
+// raising columns of the range).  Rounds of 512 columns, each
 // lane loading its 16 columns unconditionally (indices clamped into the range) before testing any, so that a round
 // costs one load latency: a search across the step of a nearly step-shaped demarcation line spans most of the node.
-__device__ __forceinline__ int global_col_search(const int32_t *__restrict__ ycol, int from, int end, int need, int R,
+__device__ __forceinline__ int global_col_search(const int32_t *__restrict__ ycol, int from, int end, int &need, int R,
                                                  int none, int lane) {
     constexpr int U = 16;
     for (int g0 = from; g0 < end; g0 += 32 * U) {
@@ -1176,12 +1201,49 @@ __device__ __forceinline__ int global_col_search(const int32_t *__restrict__ yco
     return none;
 }
 
+// warp-wide, columns in global memory with the block table of Y: as global_col_search.  The head up to the first
+// block boundary and the block where the search ends are scanned in global memory; the blocks between are
+// counted from the table, 32 per round (lane = block, a prefix sum over the lanes).
+__device__ __forceinline__ int wide_col_search(const YView &Y, int from, int cend, int need, int R, int none,
+                                               int lane) {
+    const int B = Y.B;
+    int b = (from - Y.clo + B - 1) / B;                    // first full block at or after `from`
+    const int head_end = min(cend, Y.clo + b * B);
+    if (from < head_end) {   // (on `none`, need has been reduced by the head's raising columns)
+        const int c = global_col_search(Y.g, from, head_end, need, R, none, lane);
+        if (c != none) return c;
+    }
+    const int bfull = min(Y.nblk, (cend - Y.clo) / B);   // blocks entirely below cend
+    for (; b < bfull; b += 32) {
+        const int bl = b + lane;
+        const int cnt = bl < bfull ? Y.block_count(bl, R) : 0;
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int tot = __shfl_sync(kFull, incl, 31);
+        if (tot < need) {
+            need -= tot;
+            continue;
+        }
+        const int j = __ffs(__ballot_sync(kFull, incl >= need)) - 1;
+        const int before = __shfl_sync(kFull, incl - cnt, j);
+        const int g0 = Y.clo + (b + j) * B;
+        need -= before;
+        return global_col_search(Y.g, g0, g0 + B, need, R, none, lane);
+    }
+    const int tail = max(head_end, Y.clo + bfull * B);
+    return tail < cend ? global_col_search(Y.g, tail, cend, need, R, none, lane) : none;
+}
+
 // warp-wide: one past the need-th column g in [from, cend) whose point raises delta in row R; k + 1 if none
-// (U = 0: the growing search above on staged columns; columns left in global memory always take the batched one)
+// (U = 0: the growing search above on staged columns; columns left in global memory take the block table)
 template <int U = 0>
 __device__ __forceinline__ int band_col_search(const YView &Y, int k, int from, int cend, int need, int R, int lane) {
     if (need <= 0) return from;
-    if (!Y.in_smem) return global_col_search(Y.g, from, cend, need, R, k + 1, lane);
+    if (!Y.in_smem) return wide_col_search(Y, from, cend, need, R, k + 1, lane);
     auto pred = [&](int g) {
         const int w = Y.s[g - Y.clo];
         const int y = w & kValMask;
@@ -1245,6 +1307,81 @@ __device__ __forceinline__ void band_warp_walk(int32_t *X, const YView &Y, int k
     __syncwarp();
 }
 
+// The block table of a band whose columns [clo, clo + nblk B) stay in global memory (the whole CTA; wbend zeroed
+// and S.x loaded before): per block its static raising count (one warp per run of blocks, 8 loads in flight per
+// lane), then the band's own points bucketed by block (counts, an exclusive scan over the blocks, a scatter that
+// leaves wbend[b] = end of bucket b).  `tmp`: kBandThreads ints of scratch.
+__device__ __forceinline__ void build_wide_tables(const int32_t *__restrict__ ycol, const int32_t *X, int nr, int R0,
+                                                  int clo, int B, int nblk, uint16_t *wstat, int32_t *wbend,
+                                                  uint16_t *wdyn, int32_t *tmp, int tid) {
+    constexpr int V = 8;
+    constexpr int nwarps = kBandThreads / 32;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int R1 = R0 + nr;
+    {
+        const int bw0 = (int) ((long long) nblk * warp / nwarps), bw1 = (int) ((long long) nblk * (warp + 1) / nwarps);
+        const int start = clo + bw0 * B, end = clo + bw1 * B;
+        int cur = bw0, acc = 0;
+        for (int g0 = start; g0 < end; g0 += 32 * V) {
+            int v[V];
+#pragma unroll
+            for (int u = 0; u < V; ++u) v[u] = __ldg(ycol + min(g0 + 32 * u + lane, end - 1));
+#pragma unroll
+            for (int u = 0; u < V; ++u) {
+                const int chunk = g0 + 32 * u;
+                if (chunk < end) {   // warp-uniform
+                    const int y = v[u] & kValMask;
+                    const bool st = (v[u] & kHiBit) ? (y < R0) : (y >= R1);
+                    const int cnt = __popc(__ballot_sync(kFull, st));
+                    const int blk = (chunk - clo) / B;
+                    if (blk != cur) {
+                        if (lane == 0) wstat[cur] = (uint16_t) acc;
+                        acc = 0;
+                        cur = blk;
+                    }
+                    acc += cnt;
+                }
+            }
+        }
+        if (lane == 0 && bw0 < bw1) wstat[cur] = (uint16_t) acc;
+    }
+    const int cend = clo + nblk * B;
+    for (int i = tid; i < nr; i += kBandThreads) {
+        const int c = X[i] & kValMask;
+        if (c >= clo && c < cend) atomicAdd(&wbend[(c - clo) / B], 1);
+    }
+    __syncthreads();
+    // exclusive scan of the bucket counts: a segment per thread, then the segment sums across the CTA
+    const int seg = (nblk + kBandThreads - 1) / kBandThreads;
+    const int s0 = min(nblk, tid * seg), s1 = min(nblk, s0 + seg);
+    int sum = 0;
+    for (int b = s0; b < s1; ++b) sum += wbend[b];
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) tmp[warp] = incl;
+    __syncthreads();
+    int base = incl - sum;
+    for (int w = 0; w < warp; ++w) base += tmp[w];
+    for (int b = s0; b < s1; ++b) {
+        const int c = wbend[b];
+        wbend[b] = base;
+        base += c;
+    }
+    __syncthreads();
+    for (int i = tid; i < nr; i += kBandThreads) {
+        const int v = X[i];
+        const int c = v & kValMask;
+        if (c >= clo && c < cend) {
+            const int pos = atomicAdd(&wbend[(c - clo) / B], 1);
+            wdyn[pos] = (uint16_t) (i | ((v & kHiBit) ? 0x8000 : 0));
+        }
+    }
+}
+
 // One CTA per band of kBand rows of a node: c* at every kBandSub rows (scans from the band's bottom), then
 // at every kBandWalk rows (each warp bottom-up through its sub-band), then walks of kBandWalk rows.
 __global__ void __launch_bounds__(kBandThreads, 3) sa_band_kernel(const SaNode *__restrict__ nodes,
@@ -1277,8 +1414,24 @@ __global__ void __launch_bounds__(kBandThreads, 3) sa_band_kernel(const SaNode *
         S.cst[nwalk] = cbot;
         S.nq = 0;
     }
+    // columns left in global memory: the block table (YView) in the space of the staging area
+    int B = 0, nblk = 0;
+    uint16_t *wstat = reinterpret_cast<uint16_t *>(S.y);
+    int32_t *wbend = nullptr;
+    uint16_t *wdyn = nullptr;
+    if (!ysm) {
+        B = 32 * ((ny + 32 * kWideMaxBlocks - 1) / (32 * kWideMaxBlocks));
+        nblk = ny / B;
+        wbend = reinterpret_cast<int32_t *>(wstat + ((nblk + 1) & ~1));
+        wdyn = reinterpret_cast<uint16_t *>(wbend + nblk);
+        for (int b = tid; b < nblk; b += kBandThreads) wbend[b] = 0;
+    }
     __syncthreads();
-    const YView Y{S.y, ys + nd.off, clo, ysm};
+    if (!ysm) {
+        build_wide_tables(ys + nd.off, S.x, nr, R0, clo, B, nblk, wstat, wbend, wdyn, S.queue, tid);
+        __syncthreads();
+    }
+    const YView Y{S.y, ys + nd.off, clo, ysm, wstat, wbend, wdyn, B, nblk, R0};
     // c* at the sub-band tops (warp w >= 1: row R0 + w kBandSub).  The rows between a top and the band's bottom
     // that raise delta at cbot are counted once per sub-band (each warp its own), and summed over the warps below.
     if (cbot <= k && warp * kBandSub < nr) {

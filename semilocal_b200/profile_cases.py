@@ -3,7 +3,9 @@
     python -m semilocal_b200.profile_cases batch  [pairs]     # persistent batched combing (comb_kernel)
     python -m semilocal_b200.profile_cases bit    [log2 n]    # bit-parallel combing (bit_kernel)
     python -m semilocal_b200.profile_cases wave   [log2 n]    # wavefront combing of one pair (comb_kernel)
-    python -m semilocal_b200.profile_cases hybrid [log2 n]    # hybrid: tile combing + glue tree
+    python -m semilocal_b200.profile_cases hybrid [log2 n] [tile]  # hybrid: tile combing + glue tree (tile 4096)
+    python -m semilocal_b200.profile_cases hyyro  [log2 n]    # bit-vector LLCS (hyyro_kernel)
+    python -m semilocal_b200.profile_cases plain  [n]         # one n x n pair, register-tile kernel (comb_tile_kernel)
     python -m semilocal_b200.profile_cases amatch [log2 n]    # approximate search: pattern 1000, planted text
     python -m semilocal_b200.profile_cases sa     [log2 n]    # steady ant (sa_* kernels)
     python -m semilocal_b200.profile_cases probe              # the combing roofline probe (probe_cells_kernel)
@@ -42,14 +44,20 @@ def main(argv):
         k = plan.kernel_ms()
         print(f"batch pairs={npairs} cells={cells} kernel_ms={k:.3f} gcups={cells / k / 1e6:.1f}")
         return
-    if case in ("bit", "wave", "hybrid"):
+    if case in ("bit", "wave", "hybrid", "hyyro", "plain"):
         lg = arg or 18
-        a, b = gen.hybrid_pair(1 << lg, seed=4)
+        if case == "plain":
+            a, b = gen.plain_pair(arg or 8192, seed=1)
+            lg = int(np.log2(len(a)))
+        else:
+            a, b = gen.hybrid_pair(1 << lg, seed=4)
         m, n = len(a), len(b)
         da, db = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
-        kind = {"bit": S.PLAN_BITPARALLEL, "wave": S.ALGO_WAVEFRONT, "hybrid": S.ALGO_HYBRID}[case]
-        pl = S.PairPlan(m, n, kind, tile=4096 if case == "hybrid" else 0)
-        r2 = torch.empty(m + n, dtype=torch.int32, device="cuda") if case != "bit" else None
+        kind = {"bit": S.PLAN_BITPARALLEL, "wave": S.ALGO_WAVEFRONT, "hybrid": S.ALGO_HYBRID, "hyyro": S.PLAN_HYYRO,
+                "plain": S.ALGO_WAVEFRONT}[case]
+        tile = (int(argv[3]) if len(argv) > 3 else 4096) if case == "hybrid" else 0
+        pl = S.PairPlan(m, n, kind, tile=tile)
+        r2 = torch.empty(m + n, dtype=torch.int32, device="cuda") if case not in ("bit", "hyyro") else None
         sc = torch.zeros(1, dtype=torch.int32, device="cuda")
         t0 = time.perf_counter()
         for _ in range(3):
