@@ -60,7 +60,8 @@ typedef struct slcs_opts {
     int sa_cutoff;       /* steady-ant size below which sub-problems finish in shared memory (0 = default) */
     int lane_cols;       /* wavefront of a lone pair: columns a lane combs per step -- 4 or 8 = register tiles of
                             band_rows/32 x lane_cols cells (band_rows 64..512, else 256), 1 = one column per step
-                            (the band kernel), 0 = auto: tiles of 8 x 4 up to 131072 rows unless band_rows is given */
+                            (the band kernel), 0 = auto: tiles of 8 x 4 (16 x 4 above 262144 rows) up to 524288
+                            rows unless band_rows is given */
     int reserved[2];
 } slcs_opts;
 

@@ -445,7 +445,11 @@ TileShape tile_shape_for(int rows, int band_rows, int lane_cols) {
         return TileShape{given ? band_rows / 32 : kTileRows, lane_cols};
     }
     if (lane_cols != 0 || band_rows > 0) return TileShape{};   // one column per step / the band kernel's height
-    return rows <= kTileAutoMaxRows ? TileShape{kTileRows, kTileCols} : TileShape{};
+    // automatic: 8 x 4 tiles, 16 x 4 above 2^18 rows, so that a pair keeps about 1024 bands or fewer (measured on
+    // B200, square pairs: 8192 0.61 ms against 1.0 for the band kernel, 2^18 28.8 against 46.5, 2^19 81.8 (16 x 4)
+    // against 143; at 2^20 the band kernel's 1024 bands of 1024 rows are faster: 294 against 312 or more)
+    if (rows > kTileAutoMaxRows) return TileShape{};
+    return TileShape{rows > (1 << 18) ? 16 : kTileRows, kTileCols};
 }
 
 int comb_resident_warps_sm(int num_sms) {

@@ -220,7 +220,7 @@ int launch_comb_lone(const CombPair *d_pairs, const CombItem *d_items, int nitem
 // plan_tile_bands (one height for all, the last padded with rows that never swap); R in {2, 4, 8, 16}, C in {4, 8}.
 constexpr int kTileRows = 8;                  // default tile: kTileRows x kTileCols cells per lane and step
 constexpr int kTileCols = 4;
-constexpr int kTileAutoMaxRows = 1 << 17;     // lone pairs up to this many rows take the tile kernel by default
+constexpr int kTileAutoMaxRows = 1 << 19;     // lone pairs up to this many rows take the tile kernel by default
 int plan_tile_bands(int pair, int m, int R, std::vector<CombItem> &items);
 template <typename T>
 int launch_comb_tile(const CombPair *d_pairs, const CombItem *d_items, int nitems, int *d_next, int *d_err,
@@ -228,8 +228,7 @@ int launch_comb_tile(const CombPair *d_pairs, const CombItem *d_items, int nitem
 // The tile a lone pair of `rows` rows is combed with; R = 0: the band kernel.  lane_cols is the caller's choice
 // (slcs_opts.lane_cols): 4 or 8 = the tile kernel with that width, band_rows 64..512 giving its height (else
 // kTileRows); 1 = the band kernel; 0 = automatic: the band kernel when band_rows is given, else the tile kernel up
-// to kTileAutoMaxRows rows, where its few bands leave the SMs short of warps, and the band kernel above, which
-// issues fewer instructions per cell.
+// to kTileAutoMaxRows rows (8 x 4 tiles, 16 x 4 above 2^18 rows), the band kernel above.
 struct TileShape {
     int R = 0, C = 0;
 };
