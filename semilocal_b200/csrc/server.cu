@@ -11,6 +11,8 @@
 //     resident warps, small: a quarter), so long big launches leave SMs to the small batches and their work
 //     overlaps on the device; requests that arrive while launches run are admitted into the next launch of a
 //     stream that frees up;
+//     A launch of big requests whose rows are all at most kTileAutoMaxRows combs them with the register-tile kernel
+//     (hand-off words per request, zeroed per launch), otherwise with the band kernel;
 //   * after each launch: c2r -> r2c, the request's query, 4 bytes back to the host per request;
 //   * keeps every finished braid resident (r2c, m+n int32) for further queries until it is released or
 //     evicted.
@@ -150,6 +152,7 @@ struct Req {
     int64_t need = 0;   // device bytes while in flight
     int64_t keep = 0;   // device bytes of the resident braid
     int R = 32;         // rows per lane of the request's bands
+    int tileR = 0;      // rows per lane when a launch of big requests combs it with the register-tile kernel
     int nbands = 0;
     int retries = 0;    // launches of this request that ended in a device-side wait timeout
     double t_submit = 0, t_admit = 0;
@@ -164,6 +167,7 @@ struct Launch {
     cudaEvent_t done = nullptr;
     std::vector<Req *> reqs;
     void *dmeta = nullptr;   // device: CombPair[np] | CombItem[ni] | SrvPair[np] | progress | out[np] | err | next
+    void *dhand = nullptr;   // device: the tile kernel's hand-off words (n per request), when it runs
     void *hmeta = nullptr;   // pinned mirror (out and err come back into it)
     size_t hcap = 0;
     int32_t *hout = nullptr;
@@ -280,13 +284,19 @@ int launch_group(slcs_server *S, int idx, std::vector<Req *> &reqs, int warp_cap
     cudaStream_t s = S->streams[idx];
     std::sort(reqs.begin(), reqs.end(), [](const Req *x, const Req *y) { return x->cells > y->cells; });
     const int np = (int) reqs.size();
+    // big requests of at most kTileAutoMaxRows rows comb with the register-tile kernel (few bands per request, so
+    // a warp's own latency is the bound); a launch takes it only when all its requests qualify
+    bool tile = np > 0;
+    for (const Req *r : reqs) tile = tile && r->tileR > 0;
     std::vector<CombItem> items;
     std::vector<int> prog_off(np + 1, 0);
+    std::vector<size_t> hand_off(np + 1, 0);
     for (int i = 0; i < np; ++i) {
         Req *r = reqs[i];
         int nb = 0;
-        if (r->m > 0 && r->n > 0) nb = plan_bands(i, r->m, r->R, items);
+        if (r->m > 0 && r->n > 0) nb = tile ? plan_tile_bands(i, r->m, r->tileR, items) : plan_bands(i, r->m, r->R, items);
         prog_off[i + 1] = prog_off[i] + nb;
+        hand_off[i + 1] = hand_off[i] + (tile ? (size_t) r->n : 0);
     }
     // band-major order: a request's band k is taken once its band k-1 is under way (slots are per request)
     std::stable_sort(items.begin(), items.end(), [](const CombItem &x, const CombItem &y) { return x.band < y.band; });
@@ -312,6 +322,7 @@ int launch_group(slcs_server *S, int idx, std::vector<Req *> &reqs, int warp_cap
         }
         reqs.clear();
         if (L->dmeta) dfree(L->dmeta, s);
+        if (L->dhand) dfree(L->dhand, s);
         S->pinned.put(L->hmeta, L->hcap);
         if (L->done) cudaEventDestroy(L->done);
         delete L;
@@ -319,6 +330,11 @@ int launch_group(slcs_server *S, int idx, std::vector<Req *> &reqs, int warp_cap
     };
     if (!L->hmeta) return fail_all(fail(SLCS_ERR_OOM, "pinned host allocation failed"));
     if (dalloc(&L->dmeta, bytes, s) != SLCS_OK) return fail_all(SLCS_ERR_OOM);
+    if (tile) {
+        const size_t hb = sizeof(unsigned long long) * std::max<size_t>(hand_off[np], 1);
+        if (dalloc(&L->dhand, hb, s) != SLCS_OK) return fail_all(SLCS_ERR_OOM);
+        if (cudaMemsetAsync(L->dhand, 0, hb, s) != cudaSuccess) return fail_all(fail(SLCS_ERR_CUDA, "memset failed"));
+    }
     if (cudaEventCreateWithFlags(&L->done, cudaEventDisableTiming) != cudaSuccess)
         return fail_all(fail(SLCS_ERR_CUDA, "cudaEventCreate failed"));
     unsigned char *H = static_cast<unsigned char *>(L->hmeta);
@@ -339,7 +355,8 @@ int launch_group(slcs_server *S, int idx, std::vector<Req *> &reqs, int warp_cap
             cudaMemcpyAsync(r->dab, r->ha, (size_t) r->m + r->n, cudaMemcpyHostToDevice, s) != cudaSuccess)
             return fail_all(fail(SLCS_ERR_CUDA, "input upload failed"));
         int32_t *c2r = reinterpret_cast<int32_t *>(r->dab + ab);
-        hp[i] = CombPair{r->dab, r->dab + r->m, c2r, dprog + prog_off[i], nullptr, r->m, r->n};
+        unsigned long long *hand = tile ? static_cast<unsigned long long *>(L->dhand) + hand_off[i] : nullptr;
+        hp[i] = CombPair{r->dab, r->dab + r->m, c2r, dprog + prog_off[i], nullptr, r->m, r->n, hand};
         hsp[i] = SrvPair{c2r, r->dr2c, r->m, r->n, r->q};
     }
     if (ni) std::memcpy(H + o_items, items.data(), sizeof(CombItem) * ni);
@@ -348,9 +365,11 @@ int launch_group(slcs_server *S, int idx, std::vector<Req *> &reqs, int warp_cap
         return fail_all(fail(SLCS_ERR_CUDA, "launch metadata upload failed"));
     int *derr = reinterpret_cast<int *>(D + o_err);
     // a launch of one big request that has the device to itself combs with two dependency chains per lane
-    int rc = (lone ? launch_comb_lone<uint8_t> : launch_comb<uint8_t>)(
-        reinterpret_cast<const CombPair *>(D + o_pairs), reinterpret_cast<const CombItem *>(D + o_items), ni,
-        derr + 1, derr, std::max(1, warp_cap), s);
+    const auto *dpairs = reinterpret_cast<const CombPair *>(D + o_pairs);
+    const auto *ditems = reinterpret_cast<const CombItem *>(D + o_items);
+    int rc = tile ? launch_comb_tile<uint8_t>(dpairs, ditems, ni, derr + 1, derr, std::max(1, warp_cap), kTileCols, s)
+                  : (lone ? launch_comb_lone<uint8_t> : launch_comb<uint8_t>)(dpairs, ditems, ni, derr + 1, derr,
+                                                                              std::max(1, warp_cap), s);
     if (rc != SLCS_OK) return fail_all(rc);
     int maxsize = 1;
     for (Req *r : reqs) maxsize = std::max(maxsize, r->m + r->n);
@@ -427,6 +446,7 @@ bool retire(slcs_server *S) {
         }
         for (auto it = again.rbegin(); it != again.rend(); ++it) S->pending.push_front(*it);
         dfree(L->dmeta, L->s);
+        if (L->dhand) dfree(L->dhand, L->s);
         S->pinned.put(L->hmeta, L->hcap);
         cudaEventDestroy(L->done);
         delete L;
@@ -605,7 +625,11 @@ int slcs_server_submit(slcs_server *S, const uint8_t *a, int m, const uint8_t *b
     r->cells = (int64_t) m * n;
     r->R = S->o.band_rows > 0 ? std::max(1, std::min(32, S->o.band_rows / 32)) : pick_rows_batch(m);
     r->nbands = (m > 0 && n > 0) ? (m + 32 * r->R - 1) / (32 * r->R) + 1 : 0;
-    r->need = req_need(m, n, r->nbands);
+    if (S->o.band_rows <= 0 && m > 0 && n > 0 && r->cells >= S->o.big_cells) {
+        r->tileR = tile_shape_for(m, 0, 0).R;
+        if (r->tileR > 0) r->nbands = std::max(r->nbands, (m + 32 * r->tileR - 1) / (32 * r->tileR));
+    }
+    r->need = req_need(m, n, r->nbands) + (r->tileR > 0 ? (int64_t) sizeof(unsigned long long) * n + 256 : 0);
     r->keep = (int64_t) align_up(sizeof(int32_t) * (size_t) std::max(m + n, 1), 256);
     if (r->need > S->budget) {
         delete r;
