@@ -40,7 +40,7 @@ constexpr int kSaRankSpan = 1024;  // node spans from which the moving rows are 
 constexpr int kSegW = kSaSB / 32 / (kSaThreads / 32);   // 32-row segments per warp in the rank passes
 constexpr int kSegB = 8;                                  // segments whose loads a rank pass batches
 static_assert(kSegW % kSegB == 0 && kSegB <= 32, "rank passes take whole batches");
-constexpr int kLowGroups = 2;   // 32-leaf groups a warp takes through the warp-local levels at once
+constexpr int kLowGroups = 2;   // 64-leaf nodes a warp takes through the sorting network at once
 constexpr int kWalkSpanMax = 64;   // walks crossing more columns are taken by a whole warp
 
 static_assert(kSaSB / kSaSF <= kSaThreads - 32, "the walk phase needs at least one warp without a thread walk");
@@ -279,140 +279,84 @@ __device__ __forceinline__ void warp_walk(SaShared &S, int a, int k, int top, in
     __syncwarp();
 }
 
-// One warp: the levels of spans 2..32 of the 32-leaf group at o (cnt <= 32 leaves), in registers.  Lane i
-// holds element i of the group; per level, every element's parent position is its rank in the sibling child
-// (a binary search over the sibling's sorted lanes by shuffles), the children's products are mapped to parent
-// coordinates through the group's slice of xs / ys, and c*(r) of each row comes from its definition: with
-// L(r) = #{lo points in rows >= r} = -delta(r, 0), c*(r) - 1 is the column of the L(r)-th column g of the node
-// whose point raises delta in row r (one ballot per row of the node: bit g = colind(g, r)); the lists are
-// reordered through the group's slice of PL / QL.  Only __syncwarp: nothing here is shared with other warps.
-// NG groups at once (o, o + 32, ...; group j holds cnt[j] <= 32 leaves, 0 for none): the groups' steps are
-// independent, so interleaving them hides the shuffle and shared-memory latencies of each.
+// One warp: the products of the 64-leaf nodes at o, o + 64, ... (group j holds cnt[j] <= 64 leaves, 0 for none),
+// each straight from its definition instead of through six merge levels.  The sticky product of permutations is
+// the product of the 0-Hecke monoid (Tiskin's seaweed monoid): with w = P^-1 of the node in one-line notation
+// (position = common index, value = row), bubble-sorting w by adjacent swaps s_i of inversions gives P = s_i1 s_i2
+// ... in sorting order, and R = Q * s_i1 * s_i2 * ... where "* s_i" swaps positions i, i+1 of the sequence only
+// if that adds an inversion (the combing cell's rule).  So an odd-even transposition sort of the rows over 64
+// rounds (lane l holds positions 2l, 2l+1), that swaps the carried column ranks on each of its swaps where they
+// are ascending, leaves in position i the i-th smallest row and the node-local column of its point.  Pads past
+// cnt hold INT_MAX rows and never move.  The column ranks come from counting, the sorted column list from their
+// scatter.  Only __syncwarp: the nodes belong to this warp alone.
 template <int NG>
-__device__ __forceinline__ void warp_low_levels(SaShared &S, int o, const int (&cnt)[NG], int lane) {
-    int pl[NG], ql[NG], res[NG];
-    int cmax = 0;
+__device__ __forceinline__ void warp_node64(SaShared &S, int o, const int (&cnt)[NG], int lane) {
+    int u0[NG], u1[NG], r0[NG], r1[NG], q0[NG], q1[NG];
 #pragma unroll
     for (int j = 0; j < NG; ++j) {
-        pl[j] = lane < cnt[j] ? S.PL[o + 32 * j + lane] : INT_MAX;
-        ql[j] = lane < cnt[j] ? S.QL[o + 32 * j + lane] : INT_MAX;
-        res[j] = 0;
-        cmax = max(cmax, cnt[j]);
+        const int base = o + 64 * j + 2 * lane;
+        const bool v0 = 2 * lane < cnt[j], v1 = 2 * lane + 1 < cnt[j];
+        u0[j] = v0 ? S.PL[base] : INT_MAX;
+        u1[j] = v1 ? S.PL[base + 1] : INT_MAX;
+        q0[j] = v0 ? S.QL[base] : INT_MAX;
+        q1[j] = v1 ? S.QL[base + 1] : INT_MAX;
+        r0[j] = r1[j] = 0;
+    }
+    // column ranks inside the node (the columns are distinct)
+#pragma unroll 4
+    for (int t = 0; t < 32; ++t) {
+#pragma unroll
+        for (int j = 0; j < NG; ++j) {
+            const int a = __shfl_sync(kFull, q0[j], t), b = __shfl_sync(kFull, q1[j], t);
+            r0[j] += (a < q0[j]) + (b < q0[j]);
+            r1[j] += (a < q1[j]) + (b < q1[j]);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < NG; ++j) {
+        if (2 * lane < cnt[j]) S.QL[o + 64 * j + r0[j]] = q0[j];
+        if (2 * lane + 1 < cnt[j]) S.QL[o + 64 * j + r1[j]] = q1[j];
+    }
+    const bool has_next = lane < 31, has_prev = lane > 0;
+#pragma unroll 2
+    for (int t = 0; t < 32; ++t) {
+        // even round: positions (2l, 2l + 1)
+#pragma unroll
+        for (int j = 0; j < NG; ++j) {
+            const bool c = u0[j] > u1[j];
+            const int lo = min(u0[j], u1[j]), hi = max(u0[j], u1[j]);
+            const int rmax = max(r0[j], r1[j]), rmin = min(r0[j], r1[j]);
+            u0[j] = lo;
+            u1[j] = hi;
+            r0[j] = c ? rmax : r0[j];
+            r1[j] = c ? rmin : r1[j];
+        }
+        // odd round: positions (2l + 1, 2l + 2), i.e. this lane's second with the next lane's first
+#pragma unroll
+        for (int j = 0; j < NG; ++j) {
+            const int un = __shfl_down_sync(kFull, u0[j], 1), rn = __shfl_down_sync(kFull, r0[j], 1);
+            const int up = __shfl_up_sync(kFull, u1[j], 1), rp = __shfl_up_sync(kFull, r1[j], 1);
+            const bool c1 = has_next && u1[j] > un;
+            const bool c0 = has_prev && up > u0[j];
+            r1[j] = c1 ? max(r1[j], rn) : r1[j];
+            u1[j] = c1 ? un : u1[j];
+            r0[j] = c0 ? min(rp, r0[j]) : r0[j];
+            u0[j] = c0 ? up : u0[j];
+        }
     }
 #pragma unroll
-    for (int h = 1; h < 32; h <<= 1) {
-        if (h >= cmax) break;
-        const int s = 2 * h;
-        const int a = lane & ~(s - 1);
-        int m[NG], b[NG], pp[NG], pq[NG];
-        bool two[NG], lo[NG];
-#pragma unroll
-        for (int j = 0; j < NG; ++j) {
-            m[j] = min(a + h, cnt[j]);
-            b[j] = min(a + s, cnt[j]);
-            two[j] = lane < cnt[j] && m[j] < b[j];   // the lane's node has both children
-            lo[j] = lane < m[j];
+    for (int j = 0; j < NG; ++j) {
+        const int base = o + 64 * j + 2 * lane;
+        if (2 * lane < cnt[j]) {
+            S.PL[base] = u0[j];
+            S.RES[base] = (uint16_t) r0[j];
         }
-        // parent positions in the row-id (PL) and column-id (QL) merges: the number of sibling entries below
-        // the lane's own (entries are distinct), by binary lifting over the sibling's sorted lanes
-        {
-            int sb[NG], len[NG], cp[NG], cq[NG];
-#pragma unroll
-            for (int j = 0; j < NG; ++j) {
-                sb[j] = lo[j] ? m[j] : a;
-                len[j] = lo[j] ? b[j] - m[j] : m[j] - a;
-                cp[j] = cq[j] = 0;
-            }
-#pragma unroll
-            for (int step = h; step >= 1; step >>= 1) {
-#pragma unroll
-                for (int j = 0; j < NG; ++j) {
-                    const int vp = __shfl_sync(kFull, pl[j], (sb[j] + cp[j] + step - 1) & 31);
-                    const int vq = __shfl_sync(kFull, ql[j], (sb[j] + cq[j] + step - 1) & 31);
-                    if (cp[j] + step <= len[j] && vp < pl[j]) cp[j] += step;
-                    if (cq[j] + step <= len[j] && vq < ql[j]) cq[j] += step;
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < NG; ++j) {
-                const int base = lo[j] ? lane - a : lane - m[j];
-                pp[j] = two[j] ? base + cp[j] : lane - a;
-                pq[j] = two[j] ? base + cq[j] : lane - a;
-            }
+        if (2 * lane + 1 < cnt[j]) {
+            S.PL[base + 1] = u1[j];
+            S.RES[base + 1] = (uint16_t) r1[j];
         }
-        // the child's product (row -> child-local col) in the parent's coordinates
-#pragma unroll
-        for (int j = 0; j < NG; ++j) {
-            const int cs = lo[j] ? a : m[j];
-            const int col = __shfl_sync(kFull, pq[j], (cs + res[j]) & 31);
-            if (two[j]) {
-                S.xs[o + 32 * j + a + pp[j]] = (uint16_t) (col | (lo[j] ? 0 : 0x8000));
-                S.ys[o + 32 * j + a + col] = (uint16_t) (pp[j] | (lo[j] ? 0 : 0x8000));
-            }
-        }
-        __syncwarp();
-        int x[NG], y[NG];
-#pragma unroll
-        for (int j = 0; j < NG; ++j) {
-            x[j] = two[j] ? S.xs[o + 32 * j + lane] : 0;
-            y[j] = two[j] ? S.ys[o + 32 * j + lane] : 0;
-        }
-        // c*(r) = min{c : delta(r, c) >= 0}, delta(r, 0) = -#{lo points in rows >= r}
-        const int r = lane - a;
-        // mine: bit g (warp lane of column g) = colind(g, r) for the columns of the lane's node, row r = lane - a.
-        // In row 0 the set is the node's lo columns (a lo column counts while r <= its point's row, a hi column
-        // once r is past it); going down one row flips exactly the column of the row's point.  So the set of row r
-        // is the lo columns XOR the points' columns of the rows above r: one ballot and a segmented prefix XOR
-        // over the node's lanes (log2 s shuffles) instead of one ballot per row.
-        unsigned mine[NG];
-#pragma unroll
-        for (int j = 0; j < NG; ++j) {
-            const unsigned lo_cols = __ballot_sync(kFull, two[j] && !(y[j] >> 15));
-            const unsigned own = two[j] ? (1u << (a + (x[j] & 0x7fff))) : 0u;
-            unsigned v = own;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                if (d >= s) break;
-                const unsigned t = __shfl_up_sync(kFull, v, d);
-                if (r >= d) v ^= t;
-            }
-            mine[j] = lo_cols ^ (v ^ own);
-        }
-#pragma unroll
-        for (int j = 0; j < NG; ++j) {
-            const int k = b[j] - a;
-            const unsigned lomask = __ballot_sync(kFull, two[j] && !(x[j] >> 15));
-            const unsigned upto = b[j] >= 32 ? 0xffffffffu : ((1u << b[j]) - 1u);
-            const int need = __popc(lomask & upto & ~((1u << lane) - 1u));
-            const unsigned mk = (mine[j] >> a) & (k >= 32 ? 0xffffffffu : ((1u << k) - 1u));
-            const int cstar = need == 0 ? 0 : (__popc(mk) >= need ? (int) __fns(mk, 0, need) + 1 : k + 1);
-            if (two[j]) {
-                const int xr = x[j] & 0x7fff;
-                const bool hi = x[j] >> 15;
-                const bool good = cstar >= 1 && cstar <= k && (hi ? (xr < cstar) : (xr >= cstar));
-                res[j] = good ? cstar - 1 : xr;
-            }
-        }
-        // the lists in the parent's order
-        __syncwarp();
-#pragma unroll
-        for (int j = 0; j < NG; ++j)
-            if (two[j]) {
-                S.PL[o + 32 * j + a + pp[j]] = pl[j];
-                S.QL[o + 32 * j + a + pq[j]] = ql[j];
-            }
-        __syncwarp();
-#pragma unroll
-        for (int j = 0; j < NG; ++j)
-            if (two[j]) {
-                pl[j] = S.PL[o + 32 * j + lane];
-                ql[j] = S.QL[o + 32 * j + lane];
-            }
-        __syncwarp();
     }
-#pragma unroll
-    for (int j = 0; j < NG; ++j)
-        if (lane < cnt[j]) S.RES[o + 32 * j + lane] = (uint16_t) res[j];
     __syncwarp();
 }
 
@@ -432,15 +376,15 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
         S.RES[e] = 0;
     }
     __syncthreads();
-    // spans 2..32: one warp per 32-leaf group
-    for (int o = warp * 32 * kLowGroups; o < nb; o += nwarps * 32 * kLowGroups) {
+    // spans 2..64: one warp per 64-leaf node, the product by a sorting network
+    for (int o = warp * 64 * kLowGroups; o < nb; o += nwarps * 64 * kLowGroups) {
         int cnt[kLowGroups];
 #pragma unroll
-        for (int j = 0; j < kLowGroups; ++j) cnt[j] = max(0, min(32, nb - o - 32 * j));
-        warp_low_levels<kLowGroups>(S, o, cnt, lane);
+        for (int j = 0; j < kLowGroups; ++j) cnt[j] = max(0, min(64, nb - o - 64 * j));
+        warp_node64<kLowGroups>(S, o, cnt, lane);
     }
     __syncthreads();
-    for (int size = 32; size < nb; size <<= 1) {
+    for (int size = 64; size < nb; size <<= 1) {
         const int span = size << 1;
         // ---- merge the children's lists: positions in the parent lists ----
         if (span >= 2 * kSaPerThread) {
@@ -489,6 +433,10 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
             }
             const int row = S.posP[e];
             const int col = S.posQ[cs + rc];
+            if (row >= b - a || col >= b - a) {   // positions of an inconsistent merge: report, stay in bounds
+                raise_error(err, kDevErrBadState);
+                continue;
+            }
             S.xs[a + row] = (uint16_t) (col | (hi ? 0x8000 : 0));
             S.ys[a + col] = (uint16_t) (row | (hi ? 0x8000 : 0));
         }
@@ -866,12 +814,23 @@ __global__ void __launch_bounds__(256) sa_split_kernel(const SaNode *__restrict_
 }
 
 // Merge the children's sorted lists of every node; pos receives the node-local parent position of every
-// child element (the reference's row / column mappers).  which = 0: row-id lists (splits .x), 1: column-id lists.
+// child element (the reference's row / column mappers).  blockIdx.y = 0: row-id lists (splits .x), 1: column-id
+// lists.  A CTA stages its tile's two runs in shared memory; each thread finds its own merge-path split of the
+// tile (a binary search) and merges kMerPT consecutive outputs sequentially; outputs and positions go out
+// through shared memory in coalesced stores.  The ids in a node are distinct, so the merge has no ties.
+constexpr int kMerPT = kMT / 256;
 __global__ void __launch_bounds__(256) sa_merge_kernel(const SaNode *__restrict__ nodes, const SaTile *__restrict__ tiles,
-                                                       const int2 *__restrict__ splits, int which,
-                                                       const int32_t *__restrict__ Lin, int32_t *__restrict__ Lout,
-                                                       int32_t *__restrict__ pos) {
-    __shared__ int32_t sm_lo[kMT], sm_hi[kMT];
+                                                       const int2 *__restrict__ splits,
+                                                       const int32_t *__restrict__ PLin, int32_t *__restrict__ PLout,
+                                                       int32_t *__restrict__ posP, const int32_t *__restrict__ QLin,
+                                                       int32_t *__restrict__ QLout, int32_t *__restrict__ posQ) {
+    __shared__ int32_t sm[kMT];     // the lo run [0, na), then the hi run [na, na + nbb)
+    __shared__ int32_t sout[kMT];   // merged values
+    __shared__ int32_t spos[kMT];   // parent positions of the lo run, then of the hi run
+    const int which = blockIdx.y;
+    const int32_t *__restrict__ Lin = which ? QLin : PLin;
+    int32_t *__restrict__ Lout = which ? QLout : PLout;
+    int32_t *__restrict__ pos = which ? posQ : posP;
     const SaTile tl = tiles[blockIdx.x];
     const SaNode nd = nodes[tl.node];
     const int nlo = nd.h;
@@ -884,22 +843,41 @@ __global__ void __launch_bounds__(256) sa_merge_kernel(const SaNode *__restrict_
     }
     const int32_t *lo = Lin + nd.off, *hi = Lin + nd.off + nd.h;
     const int i0 = which ? s0.y : s0.x, j0 = o0 - i0, j1 = o1 - i1;
-    const int na = i1 - i0, nbb = j1 - j0;
-    for (int x = threadIdx.x; x < na; x += blockDim.x) sm_lo[x] = lo[i0 + x];
-    for (int x = threadIdx.x; x < nbb; x += blockDim.x) sm_hi[x] = hi[j0 + x];
+    const int na = i1 - i0, nbb = j1 - j0, tot = na + nbb;
+    for (int x = threadIdx.x; x < na; x += blockDim.x) sm[x] = lo[i0 + x];
+    for (int x = threadIdx.x; x < nbb; x += blockDim.x) sm[na + x] = hi[j0 + x];
     __syncthreads();
-    for (int x = threadIdx.x; x < na; x += blockDim.x) {
-        const int v = sm_lo[x];
-        const int p = o0 + x + count_less(sm_hi, 0, nbb, v);
-        Lout[nd.off + p] = v;
-        pos[nd.off + i0 + x] = p;
+    const int d0 = threadIdx.x * kMerPT;
+    if (d0 < tot) {
+        int l = max(0, d0 - nbb), h = min(d0, na);   // the first i with lo[i] >= hi[d0 - 1 - i]
+        while (l < h) {
+            const int mid = (l + h) >> 1;
+            if (sm[mid] < sm[na + d0 - 1 - mid]) l = mid + 1;
+            else h = mid;
+        }
+        int i = l, j = d0 - l;
+        int vlo = i < na ? sm[i] : INT_MAX, vhi = j < nbb ? sm[na + j] : INT_MAX;
+        const int cnt = min(kMerPT, tot - d0);
+#pragma unroll
+        for (int t = 0; t < kMerPT; ++t) {
+            if (t < cnt) {
+                const bool take_lo = vlo < vhi;
+                sout[d0 + t] = take_lo ? vlo : vhi;
+                spos[take_lo ? i : na + j] = o0 + d0 + t;
+                if (take_lo) {
+                    ++i;
+                    vlo = i < na ? sm[i] : INT_MAX;
+                } else {
+                    ++j;
+                    vhi = j < nbb ? sm[na + j] : INT_MAX;
+                }
+            }
+        }
     }
-    for (int x = threadIdx.x; x < nbb; x += blockDim.x) {
-        const int v = sm_hi[x];
-        const int p = o0 + x + count_less(sm_lo, 0, na, v);
-        Lout[nd.off + p] = v;
-        pos[nd.off + nd.h + j0 + x] = p;
-    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < tot; x += blockDim.x) Lout[nd.off + o0 + x] = sout[x];
+    for (int x = threadIdx.x; x < na; x += blockDim.x) pos[nd.off + i0 + x] = spos[x];
+    for (int x = threadIdx.x; x < nbb; x += blockDim.x) pos[nd.off + nd.h + j0 + x] = spos[na + x];
 }
 
 // Children's products in the parent's coordinates: xs (row -> col | hi) and ys (col -> row | hi).
@@ -1800,8 +1778,8 @@ int sa_plan_run_ex(SaPlan *P, const int32_t *d_P, const int32_t *d_leafP, const 
             const SaTile *tiles = P->d_tiles + L.o_tiles;
             sa_split_kernel<<<(2 * L.ntiles + 7) / 8, 256, 0, s>>>(nodes, tiles, L.ntiles, P->pl[cur], P->ql[cur],
                                                                   P->d_splits);
-            sa_merge_kernel<<<L.ntiles, 256, 0, s>>>(nodes, tiles, P->d_splits, 0, P->pl[cur], P->pl[nxt], P->posP);
-            sa_merge_kernel<<<L.ntiles, 256, 0, s>>>(nodes, tiles, P->d_splits, 1, P->ql[cur], P->ql[nxt], P->posQ);
+            sa_merge_kernel<<<dim3((unsigned) L.ntiles, 2), 256, 0, s>>>(nodes, tiles, P->d_splits, P->pl[cur], P->pl[nxt],
+                                                                         P->posP, P->ql[cur], P->ql[nxt], P->posQ);
             sa_map_kernel<<<L.ntiles, 256, 0, s>>>(nodes, tiles, P->posP, P->posQ, P->res[cur], P->xs, P->ys, d_err);
             sa_rowhist_kernel<<<L.nl0, 256, sizeof(int32_t) * P->max_w, s>>>(nodes, P->d_tasks + L.o_l0, P->xs, P->posP,
                                                                              P->posQ, P->tab, P->vec);
@@ -1833,7 +1811,7 @@ int sa_plan_run(SaPlan *P, const int32_t *d_P, const int32_t *d_Q, int32_t *d_R,
 
 int sa_plan_launches(const SaPlan *P) {
     int c = (P->nprobtiles ? 1 : 0) + (P->nitems ? 1 : 0);
-    for (const SaLevel &L : P->levels) c += (L.nnodes ? 7 + (L.nct ? 1 : 0) + (L.nft ? 1 : 0) : 0) + (L.ncopies ? 1 : 0);
+    for (const SaLevel &L : P->levels) c += (L.nnodes ? 6 + (L.nct ? 1 : 0) + (L.nft ? 1 : 0) : 0) + (L.ncopies ? 1 : 0);
     return c;
 }
 

@@ -108,3 +108,71 @@ def test_walk_and_rank_match_the_oracle(oracle, n):
         expect = oracle.steady_ant(p, q)
         assert np.array_equal(multiply(pinv, q, combine_walk), expect), (n, s)
         assert np.array_equal(multiply(pinv, q, combine_rank, check_segments=(n <= 31)), expect), (n, s)
+
+
+def node_network(pl_leaves, ql_leaves, width=64):
+    """The shared-memory kernel's lowest node, restated lane by lane: lane l holds positions 2l, 2l+1 of a node of
+    `width` common indices (cnt <= width leaves, pads past cnt carry an infinite row).  The column ranks come from
+    counting; an odd-even transposition sort of the rows (width rounds) swaps the carried ranks on each of its
+    swaps where they are ascending (the 0-Hecke product).  Returns the sorted rows, the sorted columns and the
+    node-local product (row rank -> column rank)."""
+    inf = np.iinfo(np.int64).max
+    cnt = len(pl_leaves)
+    u = np.full(width, inf, dtype=np.int64)
+    qv = np.full(width, inf, dtype=np.int64)
+    u[:cnt], qv[:cnt] = pl_leaves, ql_leaves
+    r = np.array([int(np.sum(qv < qv[j])) for j in range(width)])
+    qs = np.full(width, inf, dtype=np.int64)
+    qs[r[:cnt]] = qv[:cnt]
+    for t in range(width):
+        for i in range(t % 2, width - 1, 2):
+            if u[i] > u[i + 1]:
+                u[i], u[i + 1] = u[i + 1], u[i]
+                if r[i] < r[i + 1]:
+                    r[i], r[i + 1] = r[i + 1], r[i]
+    return u[:cnt], qs[:cnt], r[:cnt]
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 33, 64, 100, 257])
+def test_node_network_matches_the_oracle(oracle, n):
+    """Each 64-leaf node of the bottom-up tree (the trailing one partial) by the sorting network, then the tree's
+    upper levels by the walk, gives the reference's product; and a node alone gives the product of its own
+    sub-permutations."""
+    for s in range(3):
+        p, q = gen.permutation(n, 700 + s, 1), gen.permutation(n, 750 + s, 2)
+        pinv = np.empty(n, dtype=np.int64)
+        pinv[p] = np.arange(n)
+        expect = oracle.steady_ant(p, q)
+        nodes = []
+        for o in range(0, n, 64):
+            pl, ql, res = node_network(pinv[o:o + 64], q[o:o + 64].astype(np.int64))
+            nodes.append(([int(v) for v in pl], [int(v) for v in ql], [int(v) for v in res]))
+            # the node alone: its rows and columns renumbered by rank, against the oracle's product of those
+            k = len(pl)
+            rank_r = {int(v): i for i, v in enumerate(pl)}
+            rank_c = {int(v): i for i, v in enumerate(ql)}
+            pn = np.array([rank_r[int(pinv[o + j])] for j in range(k)])
+            pn_row_to_col = np.empty(k, dtype=np.int32)
+            pn_row_to_col[pn] = np.arange(k)
+            qn = np.array([rank_c[int(q[o + j])] for j in range(k)], dtype=np.int32)
+            assert np.array_equal(np.asarray(res), oracle.steady_ant(pn_row_to_col, qn)), (n, s, o)
+        while len(nodes) > 1:
+            nxt = []
+            for i in range(0, len(nodes), 2):
+                if i + 1 == len(nodes):
+                    nxt.append(nodes[i])
+                    continue
+                (pl1, ql1, r1), (pl2, ql2, r2) = nodes[i], nodes[i + 1]
+                pl, ql = sorted(pl1 + pl2), sorted(ql1 + ql2)
+                k = len(pl)
+                xs, hi = np.zeros(k, int), np.zeros(k, bool)
+                for plc, qlc, rc, h in ((pl1, ql1, r1, False), (pl2, ql2, r2, True)):
+                    for rr, c in enumerate(rc):
+                        xs[pl.index(plc[rr])], hi[pl.index(plc[rr])] = ql.index(qlc[c]), h
+                nxt.append((pl, ql, list(combine_walk(xs, hi))))
+            nodes = nxt
+        pl, ql, res = nodes[0]
+        out = np.zeros(n, dtype=np.int32)
+        for rr in range(n):
+            out[pl[rr]] = ql[res[rr]]
+        assert np.array_equal(out, expect), (n, s)
