@@ -40,7 +40,8 @@ constexpr int kSaRankSpan = 1024;  // node spans from which the moving rows are 
 constexpr int kSegW = kSaSB / 32 / (kSaThreads / 32);   // 32-row segments per warp in the rank passes
 constexpr int kSegB = 8;                                  // segments whose loads a rank pass batches
 static_assert(kSegW % kSegB == 0 && kSegB <= 32, "rank passes take whole batches");
-constexpr int kLowGroups = 2;   // 64-leaf nodes a warp takes through the sorting network at once
+constexpr int kNodeW = 128;      // leaves of the nodes the sorting network finishes (spans 2 .. kNodeW)
+constexpr int kLowGroups = 1;   // such nodes a warp takes through the network at once
 constexpr int kWalkSpanMax = 64;   // walks crossing more columns are taken by a whole warp
 
 static_assert(kSaSB / kSaSF <= kSaThreads - 32, "the walk phase needs at least one warp without a thread walk");
@@ -279,84 +280,98 @@ __device__ __forceinline__ void warp_walk(SaShared &S, int a, int k, int top, in
     __syncwarp();
 }
 
-// One warp: the products of the 64-leaf nodes at o, o + 64, ... (group j holds cnt[j] <= 64 leaves, 0 for none),
-// each straight from its definition instead of through six merge levels.  The sticky product of permutations is
-// the product of the 0-Hecke monoid (Tiskin's seaweed monoid): with w = P^-1 of the node in one-line notation
-// (position = common index, value = row), bubble-sorting w by adjacent swaps s_i of inversions gives P = s_i1 s_i2
-// ... in sorting order, and R = Q * s_i1 * s_i2 * ... where "* s_i" swaps positions i, i+1 of the sequence only
-// if that adds an inversion (the combing cell's rule).  So an odd-even transposition sort of the rows over 64
-// rounds (lane l holds positions 2l, 2l+1), that swaps the carried column ranks on each of its swaps where they
-// are ascending, leaves in position i the i-th smallest row and the node-local column of its point.  Pads past
-// cnt hold INT_MAX rows and never move.  The column ranks come from counting, the sorted column list from their
-// scatter.  Only __syncwarp: the nodes belong to this warp alone.
-template <int NG>
-__device__ __forceinline__ void warp_node64(SaShared &S, int o, const int (&cnt)[NG], int lane) {
-    int u0[NG], u1[NG], r0[NG], r1[NG], q0[NG], q1[NG];
+// One warp: the products of the (32 E)-leaf nodes at o, o + 32 E, ... (group j holds cnt[j] <= 32 E leaves, 0 for
+// none), each straight from its definition instead of through the merge levels of spans 2 .. 32 E.  The sticky
+// product of permutations is the product of the 0-Hecke monoid (Tiskin's seaweed monoid): with w = P^-1 of the
+// node in one-line notation (position = common index, value = row), bubble-sorting w by adjacent swaps s_i of
+// inversions gives P = s_i1 s_i2 ... in sorting order, and R = Q * s_i1 * s_i2 * ... where "* s_i" swaps
+// positions i, i+1 of the sequence only if that adds an inversion (the combing cell's rule).  So an odd-even
+// transposition sort of the rows over 32 E rounds (lane l holds positions E l .. E l + E - 1), that swaps the
+// carried column ranks on each of its swaps where they are ascending, leaves in position i the i-th smallest row
+// and the node-local column of its point.  Pads past cnt hold INT_MAX rows and never move.  The column ranks come
+// from counting, the sorted column list from their scatter.  Only __syncwarp: the nodes belong to this warp alone.
+template <int E, int NG>
+__device__ __forceinline__ void warp_node(SaShared &S, int o, const int (&cnt)[NG], int lane) {
+    static_assert(E >= 2 && E % 2 == 0, "pairs of positions inside a lane");
+    constexpr int W = 32 * E;
+    int u[NG][E], r[NG][E], q[NG][E];
 #pragma unroll
-    for (int j = 0; j < NG; ++j) {
-        const int base = o + 64 * j + 2 * lane;
-        const bool v0 = 2 * lane < cnt[j], v1 = 2 * lane + 1 < cnt[j];
-        u0[j] = v0 ? S.PL[base] : INT_MAX;
-        u1[j] = v1 ? S.PL[base + 1] : INT_MAX;
-        q0[j] = v0 ? S.QL[base] : INT_MAX;
-        q1[j] = v1 ? S.QL[base + 1] : INT_MAX;
-        r0[j] = r1[j] = 0;
-    }
+    for (int j = 0; j < NG; ++j)
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int x = E * lane + e;
+            const bool v = x < cnt[j];
+            u[j][e] = v ? S.PL[o + W * j + x] : INT_MAX;
+            q[j][e] = v ? S.QL[o + W * j + x] : INT_MAX;
+            r[j][e] = 0;
+        }
     // column ranks inside the node (the columns are distinct)
-#pragma unroll 4
+#pragma unroll 2
     for (int t = 0; t < 32; ++t) {
 #pragma unroll
-        for (int j = 0; j < NG; ++j) {
-            const int a = __shfl_sync(kFull, q0[j], t), b = __shfl_sync(kFull, q1[j], t);
-            r0[j] += (a < q0[j]) + (b < q0[j]);
-            r1[j] += (a < q1[j]) + (b < q1[j]);
-        }
+        for (int j = 0; j < NG; ++j)
+#pragma unroll
+            for (int f = 0; f < E; ++f) {
+                const int a = __shfl_sync(kFull, q[j][f], t);
+#pragma unroll
+                for (int e = 0; e < E; ++e) r[j][e] += a < q[j][e];
+            }
     }
     __syncwarp();
 #pragma unroll
-    for (int j = 0; j < NG; ++j) {
-        if (2 * lane < cnt[j]) S.QL[o + 64 * j + r0[j]] = q0[j];
-        if (2 * lane + 1 < cnt[j]) S.QL[o + 64 * j + r1[j]] = q1[j];
-    }
+    for (int j = 0; j < NG; ++j)
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+            if (E * lane + e < cnt[j]) S.QL[o + W * j + r[j][e]] = q[j][e];
     const bool has_next = lane < 31, has_prev = lane > 0;
 #pragma unroll 2
-    for (int t = 0; t < 32; ++t) {
-        // even round: positions (2l, 2l + 1)
+    for (int t = 0; t < W / 2; ++t) {
+        // even round: positions (2i, 2i + 1), inside the lane
+#pragma unroll
+        for (int j = 0; j < NG; ++j)
+#pragma unroll
+            for (int e = 0; e < E; e += 2) {
+                const bool c = u[j][e] > u[j][e + 1];
+                const int lo = min(u[j][e], u[j][e + 1]), hi = max(u[j][e], u[j][e + 1]);
+                const int rmax = max(r[j][e], r[j][e + 1]), rmin = min(r[j][e], r[j][e + 1]);
+                u[j][e] = lo;
+                u[j][e + 1] = hi;
+                r[j][e] = c ? rmax : r[j][e];
+                r[j][e + 1] = c ? rmin : r[j][e + 1];
+            }
+        // odd round: positions (2i + 1, 2i + 2): inside the lane, and this lane's last with the next lane's first
 #pragma unroll
         for (int j = 0; j < NG; ++j) {
-            const bool c = u0[j] > u1[j];
-            const int lo = min(u0[j], u1[j]), hi = max(u0[j], u1[j]);
-            const int rmax = max(r0[j], r1[j]), rmin = min(r0[j], r1[j]);
-            u0[j] = lo;
-            u1[j] = hi;
-            r0[j] = c ? rmax : r0[j];
-            r1[j] = c ? rmin : r1[j];
-        }
-        // odd round: positions (2l + 1, 2l + 2), i.e. this lane's second with the next lane's first
+            const int un = __shfl_down_sync(kFull, u[j][0], 1), rn = __shfl_down_sync(kFull, r[j][0], 1);
+            const int up = __shfl_up_sync(kFull, u[j][E - 1], 1), rp = __shfl_up_sync(kFull, r[j][E - 1], 1);
 #pragma unroll
-        for (int j = 0; j < NG; ++j) {
-            const int un = __shfl_down_sync(kFull, u0[j], 1), rn = __shfl_down_sync(kFull, r0[j], 1);
-            const int up = __shfl_up_sync(kFull, u1[j], 1), rp = __shfl_up_sync(kFull, r1[j], 1);
-            const bool c1 = has_next && u1[j] > un;
-            const bool c0 = has_prev && up > u0[j];
-            r1[j] = c1 ? max(r1[j], rn) : r1[j];
-            u1[j] = c1 ? un : u1[j];
-            r0[j] = c0 ? min(rp, r0[j]) : r0[j];
-            u0[j] = c0 ? up : u0[j];
+            for (int e = 1; e + 1 < E; e += 2) {
+                const bool c = u[j][e] > u[j][e + 1];
+                const int lo = min(u[j][e], u[j][e + 1]), hi = max(u[j][e], u[j][e + 1]);
+                const int rmax = max(r[j][e], r[j][e + 1]), rmin = min(r[j][e], r[j][e + 1]);
+                u[j][e] = lo;
+                u[j][e + 1] = hi;
+                r[j][e] = c ? rmax : r[j][e];
+                r[j][e + 1] = c ? rmin : r[j][e + 1];
+            }
+            const bool c1 = has_next && u[j][E - 1] > un;
+            const bool c0 = has_prev && up > u[j][0];
+            r[j][E - 1] = c1 ? max(r[j][E - 1], rn) : r[j][E - 1];
+            u[j][E - 1] = c1 ? un : u[j][E - 1];
+            r[j][0] = c0 ? min(rp, r[j][0]) : r[j][0];
+            u[j][0] = c0 ? up : u[j][0];
         }
     }
 #pragma unroll
-    for (int j = 0; j < NG; ++j) {
-        const int base = o + 64 * j + 2 * lane;
-        if (2 * lane < cnt[j]) {
-            S.PL[base] = u0[j];
-            S.RES[base] = (uint16_t) r0[j];
+    for (int j = 0; j < NG; ++j)
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int x = E * lane + e;
+            if (x < cnt[j]) {
+                S.PL[o + W * j + x] = u[j][e];
+                S.RES[o + W * j + x] = (uint16_t) r[j][e];
+            }
         }
-        if (2 * lane + 1 < cnt[j]) {
-            S.PL[base + 1] = u1[j];
-            S.RES[base + 1] = (uint16_t) r1[j];
-        }
-    }
     __syncwarp();
 }
 
@@ -376,15 +391,15 @@ __global__ void __launch_bounds__(kSaThreads, 3) sa_block_kernel(const int32_t *
         S.RES[e] = 0;
     }
     __syncthreads();
-    // spans 2..64: one warp per 64-leaf node, the product by a sorting network
-    for (int o = warp * 64 * kLowGroups; o < nb; o += nwarps * 64 * kLowGroups) {
+    // spans 2 .. kNodeW: one warp per kNodeW-leaf node, the product by a sorting network
+    for (int o = warp * kNodeW * kLowGroups; o < nb; o += nwarps * kNodeW * kLowGroups) {
         int cnt[kLowGroups];
 #pragma unroll
-        for (int j = 0; j < kLowGroups; ++j) cnt[j] = max(0, min(64, nb - o - 64 * j));
-        warp_node64<kLowGroups>(S, o, cnt, lane);
+        for (int j = 0; j < kLowGroups; ++j) cnt[j] = max(0, min(kNodeW, nb - o - kNodeW * j));
+        warp_node<kNodeW / 32, kLowGroups>(S, o, cnt, lane);
     }
     __syncthreads();
-    for (int size = 64; size < nb; size <<= 1) {
+    for (int size = kNodeW; size < nb; size <<= 1) {
         const int span = size << 1;
         // ---- merge the children's lists: positions in the parent lists ----
         if (span >= 2 * kSaPerThread) {

@@ -133,9 +133,9 @@ def node_network(pl_leaves, ql_leaves, width=64):
     return u[:cnt], qs[:cnt], r[:cnt]
 
 
-@pytest.mark.parametrize("n", [1, 2, 7, 33, 64, 100, 257])
-def test_node_network_matches_the_oracle(oracle, n):
-    """Each 64-leaf node of the bottom-up tree (the trailing one partial) by the sorting network, then the tree's
+@pytest.mark.parametrize("width,n", [(64, 1), (64, 7), (64, 100), (128, 2), (128, 33), (128, 128), (128, 300)])
+def test_node_network_matches_the_oracle(oracle, width, n):
+    """Each node of `width` leaves of the bottom-up tree (the trailing one partial) by the sorting network, then the tree's
     upper levels by the walk, gives the reference's product; and a node alone gives the product of its own
     sub-permutations."""
     for s in range(3):
@@ -144,8 +144,8 @@ def test_node_network_matches_the_oracle(oracle, n):
         pinv[p] = np.arange(n)
         expect = oracle.steady_ant(p, q)
         nodes = []
-        for o in range(0, n, 64):
-            pl, ql, res = node_network(pinv[o:o + 64], q[o:o + 64].astype(np.int64))
+        for o in range(0, n, width):
+            pl, ql, res = node_network(pinv[o:o + width], q[o:o + width].astype(np.int64), width)
             nodes.append(([int(v) for v in pl], [int(v) for v in ql], [int(v) for v in res]))
             # the node alone: its rows and columns renumbered by rank, against the oracle's product of those
             k = len(pl)
