@@ -289,7 +289,8 @@ __device__ __forceinline__ void warp_walk(SaShared &S, int a, int k, int top, in
 // transposition sort of the rows over 32 E rounds (lane l holds positions E l .. E l + E - 1), that swaps the
 // carried column ranks on each of its swaps where they are ascending, leaves in position i the i-th smallest row
 // and the node-local column of its point.  Pads past cnt hold INT_MAX rows and never move.  The column ranks come
-// from counting, the sorted column list from their scatter.  Only __syncwarp: the nodes belong to this warp alone.
+// from counting inside each half of the node and a binary search of the other half; the sorted column list is
+// their scatter.  Only __syncwarp: the nodes belong to this warp alone.
 template <int E, int NG>
 __device__ __forceinline__ void warp_node(SaShared &S, int o, const int (&cnt)[NG], int lane) {
     static_assert(E >= 2 && E % 2 == 0, "pairs of positions inside a lane");
@@ -305,17 +306,41 @@ __device__ __forceinline__ void warp_node(SaShared &S, int o, const int (&cnt)[N
             q[j][e] = v ? S.QL[o + W * j + x] : INT_MAX;
             r[j][e] = 0;
         }
-    // column ranks inside the node (the columns are distinct)
+    // column ranks inside the node (the columns are distinct): inside the lane's half of the node (16 lanes) by
+    // counting, plus the other half's columns below by a binary search of that half's sorted columns
+    constexpr int H = W / 2;   // positions per half
+    const int hb = lane & 16;  // first lane of this lane's half
 #pragma unroll 2
-    for (int t = 0; t < 32; ++t) {
+    for (int t = 0; t < 16; ++t) {
 #pragma unroll
         for (int j = 0; j < NG; ++j)
 #pragma unroll
             for (int f = 0; f < E; ++f) {
-                const int a = __shfl_sync(kFull, q[j][f], t);
+                const int a = __shfl_sync(kFull, q[j][f], hb + t);
 #pragma unroll
                 for (int e = 0; e < E; ++e) r[j][e] += a < q[j][e];
             }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < NG; ++j)
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+            if (E * lane + e < cnt[j]) S.QL[o + W * j + (hb ? H : 0) + r[j][e]] = q[j][e];
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < NG; ++j) {
+        const int other = hb ? 0 : H;   // the other half's first position
+        const int nother = min(H, max(0, cnt[j] - other));
+        const int32_t *arr = S.QL + o + W * j + other;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            int pos = 0;   // entries of arr[0, nother) below q
+#pragma unroll
+            for (int st = H; st > 0; st >>= 1)
+                if (pos + st <= nother && arr[pos + st - 1] < q[j][e]) pos += st;
+            r[j][e] += pos;
+        }
     }
     __syncwarp();
 #pragma unroll
