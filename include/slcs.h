@@ -48,7 +48,8 @@ extern "C" {
 #define SLCS_ERR_BUSY 8         /* server queue full / request not finished */
 
 /* ---- algorithm selection ------------------------------------------------------------------------ */
-#define SLCS_ALGO_AUTO 0        /* engine chooses: wavefront; hybrid (65536-tiles) once both lengths reach 2^19 */
+#define SLCS_ALGO_AUTO 0        /* engine chooses: wavefront; the hybrid once both lengths reach 2^17, tiles of about
+                                   min(m, n) / 16 (a power of two in [16384, 65536]) */
 #define SLCS_ALGO_WAVEFRONT 1   /* tiled wavefront combing over the whole grid */
 #define SLCS_ALGO_HYBRID 2      /* tiles combed independently, glued by GPU steady ant */
 

@@ -138,8 +138,16 @@ int comb_wavefront_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int3
     return check_dev_err(err.p, s);
 }
 
-constexpr int kAutoTile = 1 << 16;         // tile edge of the hybrid the engine chooses by itself
-constexpr int kAutoHybridMin = 1 << 19;    // both lengths at least this: AUTO takes the hybrid
+constexpr int kAutoHybridMin = 1 << 17;    // both lengths at least this: AUTO takes the hybrid
+
+// Tile edge of the hybrid the engine chooses by itself: about a sixteenth of the shorter length, a power of two in
+// [2^14, 2^16] -- enough tiles to fill the device with bands, few enough glue levels.
+int auto_tile(int m, int n) {
+    const int want = std::min(m, n) / 16;
+    int t = 1 << 14;
+    while (t < want && t < (1 << 16)) t <<= 1;
+    return t;
+}
 
 // The last hybrid plan of each device, kept for the next call of the same shape (planning a hybrid -- tile
 // descriptors, glue levels, steady-ant plans, scratch -- costs far more host time than running a small one).  A
@@ -155,11 +163,12 @@ HybridCache g_hcache[64];
 template <typename T>
 int comb_hybrid_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int32_t *d_r2c, int32_t *d_c2r,
                     int32_t *d_score, const slcs_opts *opts, cudaStream_t s) {
-    // tiles: the caller's, else for the engine's own choice of the hybrid (AUTO, large pairs) kAutoTile, else the
+    // tiles: the caller's, else for the engine's own choice of the hybrid (AUTO, large pairs) auto_tile, else the
     // tuned edge
     const bool chosen = !opts || opts->algo == SLCS_ALGO_AUTO;
-    const int tr = (opts && opts->tile_rows > 0) ? opts->tile_rows : (chosen ? kAutoTile : pick_tile());
-    const int tc = (opts && opts->tile_cols > 0) ? opts->tile_cols : (chosen ? kAutoTile : pick_tile());
+    const int at = auto_tile(m, n);
+    const int tr = (opts && opts->tile_rows > 0) ? opts->tile_rows : (chosen ? at : pick_tile());
+    const int tc = (opts && opts->tile_cols > 0) ? opts->tile_cols : (chosen ? at : pick_tile());
     HybridCache &C = g_hcache[E->device];
     HybridPlan *H = nullptr;
     bool from_cache = false;
@@ -213,9 +222,10 @@ int comb_hybrid_dev(Engine *E, const T *d_a, int m, const T *d_b, int n, int32_t
 }
 
 // Algorithm choice: the hybrid when asked for, or (AUTO) for grids large in both dimensions, with tiles of
-// kAutoTile x kAutoTile: few enough glue levels (8 at 2^20) that the full occupancy of the tile combing outweighs
-// them.  Measured on B200, the 2^20 pair: hybrid with 65536-tiles 240 ms, wavefront 270-300 ms, hybrid with
-// 4096-tiles 370 ms (16 glue levels).
+// auto_tile(m, n): few enough glue levels that the full occupancy of the tile combing outweighs them.  Measured on
+// B200 (event-timed, random and similar-string pairs alike): 2^17 pair wavefront 9.6 ms, 16384-tiles 7.2 (8192:
+// 7.9, 32768: 8.9); 2^18 pair 28.8 ms, 16384-tiles 18.9 (65536: 19.5); 2^19 pair 81.6 ms, 32768-tiles 58.0
+// (16384: 61.0, 65536: 61.3); 2^20 pair 300 ms, 65536-tiles 207, 4096-tiles 309 (16 glue levels).
 bool use_hybrid(const slcs_opts *opts, int m, int n) {
     const int algo = opts ? opts->algo : SLCS_ALGO_AUTO;
     if (algo == SLCS_ALGO_HYBRID) return true;

@@ -97,3 +97,21 @@ def test_cached_plan_outlives_the_callers_stream(engine, oracle):
            oracle.comb_antidiag(*first, 4)]
     for k, (g, e) in enumerate(zip(got, exp)):
         assert np.array_equal(g, e), k
+
+
+@pytest.mark.parametrize("m,n,similar", [(1 << 17, 1 << 17, False), (150001, 140003, True), (140003, 262147, False)])
+def test_auto_takes_the_hybrid_and_matches_the_oracle(engine, oracle, m, n, similar):
+    """AUTO takes the hybrid once both lengths reach 2^17 (tiles of about min(m, n) / 16, here 16384; ragged edges,
+    both orientations): bit-exact against the oracle and against the wavefront forced by the caller."""
+    if similar:
+        a, b = gen.hybrid_pair(max(m, n), seed=9)
+        a, b = a[:m], b[:n]
+    else:
+        rng = np.random.default_rng(m + 3 * n)
+        a, b = _rand(rng, m, 4), _rand(rng, n, 4)
+    r2c, score = engine.comb(a, b)
+    exp = oracle.comb_antidiag(a, b, os.cpu_count() or 8)
+    assert np.array_equal(r2c, exp)
+    assert score == oracle.global_score(exp, m, n)
+    w, sw = engine.comb(a, b, algo=engine.ALGO_WAVEFRONT)
+    assert np.array_equal(w, exp) and sw == score
