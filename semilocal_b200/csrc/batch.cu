@@ -1,8 +1,9 @@
 // batch.cu -- batched combing of many independent pairs: one persistent, length-bucketed launch.
 //
 // Work items are (pair, band) with a per-item band height 32*R (R from the pair's length: long pairs use
-// R = 32, the last band of a pair the smallest height covering it); items are ordered longest pair first
-// (LPT) with a pair's bands consecutive, and persistent warps dequeue them in that order.  The device step
+// R = 32, the last band of a pair the smallest height covering it); items are ordered by a target start time
+// (band k of a pair at k times its share of the launch, first bands by decreasing pair cost), and persistent
+// warps dequeue them in that order.  The device step
 // (counter resets, the combing launch, the end->start inversion) can be captured once in a CUDA graph and
 // replayed.  Mode 1 issues one launch per pair instead (the per-pair baseline on the same plan).
 #include <algorithm>
@@ -144,11 +145,31 @@ int slcs_batch_create(const int32_t *m, const int32_t *n, int npairs, int mode, 
         }
     }
     if (mode == 0) {
-        // band-major order (all first bands by decreasing pair cost, then all second bands, ...): a warp takes
-        // band k of a pair only after band k-1 of it is well under way, instead of idling behind it.  A band still
-        // waits only on a band taken earlier, so no assumption about co-residency is added.
-        std::stable_sort(bt->items.begin(), bt->items.end(),
-                         [](const CombItem &x, const CombItem &y) { return x.band < y.band; });
+        // Work order: band k of pair p gets the target start k (T - D_p) / B_p, with D_p the time of its longest
+        // band (columns x band height), B_p its band count and T the launch's work over the resident warps; ties by
+        // band index, then by decreasing pair cost (every pair's first band comes first).  A pair's bands are
+        // spread over the launch so that its last band starts early enough to end with it (plain band-major order
+        // leaves the late bands of the longest pairs, each a long item, for the very end), while consecutive bands
+        // of a pair stay far apart in the order, so a warp takes band k only after band k-1 is well under way
+        // instead of polling behind it.  A band still waits only on a band taken earlier: no assumption about
+        // co-residency is added.
+        const double W = std::max(1, comb_resident_warps(E));
+        std::vector<int> nb(npairs, 0);
+        std::vector<double> gap(npairs, 0.0);
+        double work = 0;
+        for (const CombItem &it : bt->items) {
+            const double d = (double) (bt->n[it.pair] + 32) * 32.0 * it.R;
+            nb[it.pair]++;
+            gap[it.pair] = std::max(gap[it.pair], d);
+            work += d;
+        }
+        for (int p = 0; p < npairs; ++p)
+            if (nb[p]) gap[p] = std::max(work / W - gap[p], 0.0) / nb[p];
+        std::stable_sort(bt->items.begin(), bt->items.end(), [&](const CombItem &x, const CombItem &y) {
+            const double kx = x.band * gap[x.pair], ky = y.band * gap[y.pair];
+            if (kx != ky) return kx < ky;
+            return x.band < y.band;
+        });
         bt->item_begin.push_back((int) bt->items.size());
     }
     bt->resident = comb_resident_warps(E);
