@@ -17,11 +17,13 @@
 // 1 <= c*(r) <= k and the row's point lies on the wrong side of c*(r) (a hi point left of it or a lo point at
 // or right of it): there the point moves to column c*(r) - 1 (the reference's "good points").  Row by row,
 // c*(r) = c*(r+1) unless row r's point flips the sign, else one past the next column whose point raises
-// delta(r, .).  c* at every 32nd row is found by warp-wide ballot scans.  Below 2^12 (shared memory) the rows
-// between are not walked: c* is non-increasing in r and the product is a permutation, so the moving rows take
-// exactly their own columns, the topmost row the largest, and a row moves iff the sign of delta(r, x_r) says
-// so; that sign comes from the c* of the row's 32-row segment and two short counts.  At the HBM levels the rows
-// between are walked by one thread (or, for a long column span, one warp) each.
+// delta(r, .).  c* at every 32nd row is found by warp-wide ballot scans.  Inside a CTA's shared-memory subtree (up
+// to 2^12 common indices) the nodes of up to kNodeW leaves come straight from the product's definition as a
+// 0-Hecke product, by a sorting network (warp_node); spans up to 512 walk the rows between the 32-row boundaries;
+// from span 1024 those rows are not walked: c* is non-increasing in r and the product is a permutation, so the
+// moving rows take exactly their own columns, the topmost row the largest, and a row moves iff the sign of
+// delta(r, x_r) says so; that sign comes from the c* of the row's 32-row segment and two short counts.  At the
+// HBM levels the rows between are walked by one thread (or, for a long column span, one warp) each.
 #include <algorithm>
 #include <climits>
 #include <numeric>
