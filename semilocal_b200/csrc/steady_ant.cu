@@ -886,8 +886,19 @@ __global__ void __launch_bounds__(256) sa_merge_kernel(const SaNode *__restrict_
     const int32_t *lo = Lin + nd.off, *hi = Lin + nd.off + nd.h;
     const int i0 = which ? s0.y : s0.x, j0 = o0 - i0, j1 = o1 - i1;
     const int na = i1 - i0, nbb = j1 - j0, tot = na + nbb;
-    for (int x = threadIdx.x; x < na; x += blockDim.x) sm[x] = lo[i0 + x];
-    for (int x = threadIdx.x; x < nbb; x += blockDim.x) sm[na + x] = hi[j0 + x];
+    {   // the two runs: all of a thread's loads are issued before any of them is used (one load latency per CTA)
+        int v[kMerPT];
+#pragma unroll
+        for (int u = 0; u < kMerPT; ++u) {
+            const int x = threadIdx.x + 256 * u;
+            v[u] = x < na ? lo[i0 + x] : (x < tot ? hi[j0 + x - na] : 0);
+        }
+#pragma unroll
+        for (int u = 0; u < kMerPT; ++u) {
+            const int x = threadIdx.x + 256 * u;
+            if (x < tot) sm[x] = v[u];
+        }
+    }
     __syncthreads();
     const int d0 = threadIdx.x * kMerPT;
     if (d0 < tot) {
@@ -927,21 +938,36 @@ __global__ void __launch_bounds__(256) sa_map_kernel(const SaNode *__restrict__ 
                                                      const int32_t *__restrict__ posP, const int32_t *__restrict__ posQ,
                                                      const int32_t *__restrict__ RES, int32_t *__restrict__ xs,
                                                      int32_t *__restrict__ ys, int *err) {
+    // 256 threads, kMT / 256 elements each; every round of loads is issued before its values are used
+    constexpr int U = kMT / 256;
     const SaTile tl = tiles[blockIdx.x];
     const SaNode nd = nodes[tl.node];
     const int e0 = tl.t * kMT, e1 = min(e0 + kMT, nd.k);
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    int rc[U], row[U], col[U];
+    bool ok[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int e = e0 + threadIdx.x + 256 * u;
+        ok[u] = e < e1;
+        rc[u] = ok[u] ? RES[nd.off + e] : 0;
+        row[u] = ok[u] ? posP[nd.off + e] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int e = e0 + threadIdx.x + 256 * u;
         const bool hi = e >= nd.h;
-        const int cs = hi ? nd.h : 0;
-        const int rc = RES[nd.off + e];
-        if (rc < 0 || rc >= (hi ? nd.k - nd.h : nd.h)) {
+        if (ok[u] && (rc[u] < 0 || rc[u] >= (hi ? nd.k - nd.h : nd.h))) {
             raise_error(err, kDevErrBadState);
-            continue;
+            ok[u] = false;
         }
-        const int row = posP[nd.off + e];
-        const int col = posQ[nd.off + cs + rc];
-        xs[nd.off + row] = col | (hi ? kHiBit : 0);
-        ys[nd.off + col] = row | (hi ? kHiBit : 0);
+        col[u] = ok[u] ? posQ[nd.off + (hi ? nd.h : 0) + rc[u]] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        if (!ok[u]) continue;
+        const bool hi = e0 + (int) threadIdx.x + 256 * u >= nd.h;
+        xs[nd.off + row[u]] = col[u] | (hi ? kHiBit : 0);
+        ys[nd.off + col[u]] = row[u] | (hi ? kHiBit : 0);
     }
 }
 
