@@ -1007,10 +1007,19 @@ __global__ void __launch_bounds__(256) sa_rowhist_kernel(const SaNode *__restric
         vec[nd.vec_off + nd.NR + 1 + h] = lower_bound_g(posQ + nd.off, nd.h, (int) min((int64_t) h * nd.Sc, (int64_t) INT_MAX));
     if (g < nd.NR) {
         const int r0 = g * nd.Sr, r1 = min(r0 + nd.Sr, nd.k);
-        for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-            const int v = xs[nd.off + r];
-            const int hh = (v & kValMask) / nd.Sc;
-            if (hh < W) atomicAdd(&hist[hh], (v & kHiBit) ? 1 : -1);
+        for (int rb = r0; rb < r1; rb += 8 * (int) blockDim.x) {   // eight loads in flight per thread
+            int v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int r = rb + (int) threadIdx.x + (int) blockDim.x * u;
+                v[u] = r < r1 ? xs[nd.off + r] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                if (v[u] < 0) continue;
+                const int hh = (v[u] & kValMask) / nd.Sc;
+                if (hh < W) atomicAdd(&hist[hh], (v[u] & kHiBit) ? 1 : -1);
+            }
         }
     }
     __syncthreads();
@@ -1452,9 +1461,30 @@ __global__ void __launch_bounds__(kBandThreads, 3) sa_band_kernel(const SaNode *
     const int ny = cend - clo;
     const bool ysm = ny <= kBandYCap;
     const int nwalk = (nr + kBandWalk - 1) / kBandWalk;
-    for (int i = tid; i < nr; i += kBandThreads) S.x[i] = xs[nd.off + R0 + i];
+    // staging, eight loads in flight per thread
+    for (int i0 = 0; i0 < nr; i0 += 8 * kBandThreads) {
+        int v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + tid + kBandThreads * u;
+            v[u] = i < nr ? xs[nd.off + R0 + i] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (i0 + tid + kBandThreads * u < nr) S.x[i0 + tid + kBandThreads * u] = v[u];
+    }
     if (ysm)
-        for (int i = tid; i < ny; i += kBandThreads) S.y[i] = ys[nd.off + clo + i];
+        for (int i0 = 0; i0 < ny; i0 += 8 * kBandThreads) {
+            int v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int i = i0 + tid + kBandThreads * u;
+                v[u] = i < ny ? ys[nd.off + clo + i] : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (i0 + tid + kBandThreads * u < ny) S.y[i0 + tid + kBandThreads * u] = v[u];
+        }
     if (tid == 0) {
         S.cst[0] = ctop;
         S.cst[nwalk] = cbot;
